@@ -1,0 +1,746 @@
+/*
+ * The device object and the acDevice* C ABI (include/astaroth_b200.h).
+ *
+ * Reference: src/core/device.cc (struct device_s :63-74, acDeviceCreate
+ * :509-594, acDeviceDestroy :602-630, swaps :635-663, load/store :666-854,
+ * acDeviceIntegrateSubstep :941-997, boundconds :999-1017, reductions
+ * :1370-1481) and the buffer allocation of acVBACreate
+ * (acc-runtime/api/vba.cc:313-488).
+ *
+ * B200 design: the 8 fields of each buffer are one contiguous allocation
+ * (SoA, x fastest, halos included, exactly the host layout so load/store are
+ * single copies); every API call returns an AcResult instead of aborting;
+ * kernel parameters travel by value (no __constant__ state), so several
+ * devices and CUDA graphs coexist without global singletons.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "internal.h"
+
+static const char* kVersion = "astaroth_b200 0.1 (sm_100a)";
+
+/* ------------------------------------------------------------------------- */
+
+Geom
+ac_make_geom(const AcMeshInfo& info)
+{
+    Geom g;
+    const int3 n = info.int3_params[AC_nlocal];
+    g.nx         = n.x;
+    g.ny         = n.y;
+    g.nz         = n.z;
+    g.mx         = n.x + 2 * NGHOST;
+    g.my         = n.y + 2 * NGHOST;
+    g.mz         = n.z + 2 * NGHOST;
+    g.mxy        = (long long)g.mx * g.my;
+    g.cells      = g.mxy * g.mz;
+    return g;
+}
+
+void
+ac_make_stencil(const AcMeshInfo& info, StencilCoef* sc)
+{
+    const double c[3] = {3.0 / 4.0, -3.0 / 20.0, 1.0 / 60.0};
+    const double d[4] = {-49.0 / 18.0, 3.0 / 2.0, -3.0 / 20.0, 1.0 / 90.0};
+    const double e[3] = {270.0 / 720.0, -27.0 / 720.0, 2.0 / 720.0};
+    const AcReal3 inv = info.real3_params[AC_inv_ds];
+    const double iv[3] = {inv.x, inv.y, inv.z};
+    for (int a = 0; a < 3; ++a) {
+        for (int k = 0; k < 3; ++k)
+            sc->d1[a][k] = c[k] * iv[a];
+        for (int k = 0; k < 4; ++k)
+            sc->d2[a][k] = d[k] * iv[a] * iv[a];
+    }
+    const int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2};
+    for (int m = 0; m < 3; ++m)
+        for (int k = 0; k < 3; ++k)
+            sc->mix[m][k] = e[k] * iv[pa[m]] * iv[pb[m]];
+}
+
+void
+ac_make_phys(const AcMeshInfo& info, PhysConst* pc)
+{
+    const double* r  = info.real_params;
+    pc->nu           = r[AC_nu_visc];
+    pc->eta          = r[AC_eta];
+    pc->zeta         = r[AC_zeta];
+    pc->inv_mu0      = 1.0 / r[AC_mu0];
+    pc->eta_mu0      = r[AC_eta] * r[AC_mu0];
+    pc->cs2_sound    = r[AC_cs_sound] * r[AC_cs_sound];
+    pc->gamma        = r[AC_gamma];
+    pc->gamma_m1     = r[AC_gamma] - 1.0;
+    pc->inv_cp       = 1.0 / r[AC_cp_sound];
+    pc->gamma_inv_cp = r[AC_gamma] / r[AC_cp_sound];
+    pc->lnrho0       = r[AC_lnrho0];
+    pc->inv_exp_lnT0 = exp(-r[AC_lnT0]);
+    pc->K            = r[AC_K_heatcond];
+}
+
+static bool
+stream_ok(const Stream s)
+{
+    return (int)s >= 0 && (int)s < NUM_STREAMS;
+}
+
+static void
+invalidate_graphs(Device d)
+{
+    for (int s = 0; s < NUM_STREAMS; ++s)
+        for (int p = 0; p < 2; ++p) {
+            if (d->graphs[s][p].valid)
+                cudaGraphExecDestroy(d->graphs[s][p].exec);
+            d->graphs[s][p].valid = 0;
+        }
+}
+
+static void
+release(Device d)
+{
+    if (!d)
+        return;
+    cudaSetDevice(d->id);
+    cudaDeviceSynchronize();
+    invalidate_graphs(d);
+    cudaFree(d->in_block);
+    cudaFree(d->out_block);
+    cudaFree(d->red.partials);
+    cudaFreeHost(d->host_result);
+    for (int s = 0; s < NUM_STREAMS; ++s)
+        if (d->streams[s])
+            cudaStreamDestroy(d->streams[s]);
+    free(d);
+}
+
+/* ------------------------------------------------------------------------- */
+
+extern "C" const char*
+acB200Version(void)
+{
+    return kVersion;
+}
+
+extern "C" AcResult
+acDeviceCreate(const int id, const AcMeshInfo device_config, Device* device_handle)
+{
+    if (!device_handle)
+        return AC_FAILURE;
+    *device_handle = NULL;
+    int count      = 0;
+    AC_CUDA_CHECK(cudaGetDeviceCount(&count));
+    if (id < 0 || id >= count) {
+        fprintf(stderr, "astaroth_b200: device id %d out of range (%d devices)\n", id, count);
+        return AC_FAILURE;
+    }
+    AC_CUDA_CHECK(cudaSetDevice(id));
+
+    AcMeshInfo info = device_config;
+    if (acHostUpdateParams(&info) != AC_SUCCESS) {
+        fprintf(stderr, "astaroth_b200: invalid AcMeshInfo (AC_ngrid and AC_ds must be > 0)\n");
+        return AC_FAILURE;
+    }
+    const int precision = info.int_params[AC_precision];
+    if (precision != 0) {
+        fprintf(stderr, "astaroth_b200: AC_precision=%d is not supported by this build\n",
+                precision);
+        return AC_FAILURE;
+    }
+
+    device_s* d = (device_s*)calloc(1, sizeof(device_s));
+    if (!d)
+        return AC_FAILURE;
+    d->id        = id;
+    d->config    = info;
+    d->geom      = ac_make_geom(info);
+    d->precision = precision;
+    d->solve_variant = info.int_params[AC_debug_plain_kernel] ? 0 : 1;
+
+#define CREATE_CHECK(call)                                                                    \
+    do {                                                                                      \
+        const cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess) {                                                              \
+            fprintf(stderr, "astaroth_b200: %s failed: %s\n", #call, cudaGetErrorString(e_)); \
+            release(d);                                                                       \
+            return AC_FAILURE;                                                                \
+        }                                                                                     \
+    } while (0)
+
+    for (int s = 0; s < NUM_STREAMS; ++s)
+        CREATE_CHECK(cudaStreamCreateWithFlags(&d->streams[s], cudaStreamNonBlocking));
+
+    const size_t bytes = (size_t)AC_NF * (size_t)d->geom.cells * sizeof(double);
+    CREATE_CHECK(cudaMalloc((void**)&d->in_block, bytes));
+    CREATE_CHECK(cudaMalloc((void**)&d->out_block, bytes));
+    for (int q = 0; q < AC_NF; ++q) {
+        d->f.in[q]  = d->in_block + (size_t)q * d->geom.cells;
+        d->f.out[q] = d->out_block + (size_t)q * d->geom.cells;
+    }
+    /* zero-filled in and out, as acVBAReset (acc-runtime/api/vba.cc:274-307) */
+    CREATE_CHECK(cudaMemsetAsync(d->in_block, 0, bytes, d->streams[0]));
+    CREATE_CHECK(cudaMemsetAsync(d->out_block, 0, bytes, d->streams[0]));
+
+    const int blocks    = ac_reduce_blocks(d->geom);
+    d->red.max_blocks   = blocks;
+    const size_t rbytes = (2 * (size_t)blocks + 2) * sizeof(double) + 64;
+    CREATE_CHECK(cudaMalloc((void**)&d->red.partials, rbytes));
+    CREATE_CHECK(cudaMemsetAsync(d->red.partials, 0, rbytes, d->streams[0]));
+    d->red.result  = d->red.partials + 2 * (size_t)blocks;
+    d->red.counter = (unsigned int*)(d->red.result + 2);
+    CREATE_CHECK(cudaMallocHost((void**)&d->host_result, sizeof(double)));
+    CREATE_CHECK(cudaStreamSynchronize(d->streams[0]));
+#undef CREATE_CHECK
+
+    *device_handle = d;
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceDestroy(Device* device_handle)
+{
+    if (!device_handle)
+        return AC_FAILURE;
+    if (!*device_handle)
+        return AC_SUCCESS;
+    release(*device_handle);
+    *device_handle = NULL;
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDevicePrintInfo(const Device d)
+{
+    if (!d)
+        return AC_FAILURE;
+    cudaDeviceProp p;
+    AC_CUDA_CHECK(cudaGetDeviceProperties(&p, d->id));
+    printf("astaroth_b200 device %d: %s, sm_%d%d, %d SMs, %.1f GiB\n", d->id, p.name, p.major,
+           p.minor, p.multiProcessorCount, (double)p.totalGlobalMem / (1 << 30));
+    printf("  mesh: n = (%d, %d, %d), m = (%d, %d, %d), precision %s\n", d->geom.nx, d->geom.ny,
+           d->geom.nz, d->geom.mx, d->geom.my, d->geom.mz, d->precision ? "fp32-comp" : "fp64");
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceSynchronizeStream(const Device d, const Stream stream)
+{
+    if (!d)
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    if (stream == STREAM_ALL) {
+        for (int s = 0; s < NUM_STREAMS; ++s)
+            AC_CUDA_CHECK(cudaStreamSynchronize(d->streams[s]));
+        return AC_SUCCESS;
+    }
+    if (!stream_ok(stream))
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaStreamSynchronize(d->streams[stream]));
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceSwapBuffer(const Device d, const VertexBufferHandle h)
+{
+    if (!d || (int)h < 0 || h >= NUM_VTXBUF_HANDLES)
+        return AC_FAILURE;
+    double* t   = d->f.in[h];
+    d->f.in[h]  = d->f.out[h];
+    d->f.out[h] = t;
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceSwapBuffers(const Device d)
+{
+    if (!d)
+        return AC_FAILURE;
+    for (int q = 0; q < AC_NF; ++q)
+        acDeviceSwapBuffer(d, (VertexBufferHandle)q);
+    return AC_SUCCESS;
+}
+
+/* ---- uniforms / config ---- */
+
+static AcResult
+refresh_config(Device d, const AcMeshInfo& info)
+{
+    AcMeshInfo next = info;
+    if (acHostUpdateParams(&next) != AC_SUCCESS)
+        return AC_FAILURE;
+    const Geom g = ac_make_geom(next);
+    if (g.nx != d->geom.nx || g.ny != d->geom.ny || g.nz != d->geom.nz) {
+        fprintf(stderr, "astaroth_b200: mesh dimensions cannot change after acDeviceCreate\n");
+        return AC_FAILURE;
+    }
+    if (next.int_params[AC_precision] != d->precision) {
+        fprintf(stderr, "astaroth_b200: AC_precision cannot change after acDeviceCreate\n");
+        return AC_FAILURE;
+    }
+    d->config = next;
+    invalidate_graphs(d);
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceLoadScalarUniform(const Device d, const Stream stream, const AcRealParam param,
+                          const AcReal value)
+{
+    (void)stream;
+    if (!d || (int)param < 0 || param >= NUM_REAL_PARAMS)
+        return AC_FAILURE;
+    AcMeshInfo info         = d->config;
+    info.real_params[param] = value;
+    return refresh_config(d, info);
+}
+
+extern "C" AcResult
+acDeviceLoadVectorUniform(const Device d, const Stream stream, const AcReal3Param param,
+                          const AcReal3 value)
+{
+    (void)stream;
+    if (!d || (int)param < 0 || param >= NUM_REAL3_PARAMS)
+        return AC_FAILURE;
+    AcMeshInfo info          = d->config;
+    info.real3_params[param] = value;
+    return refresh_config(d, info);
+}
+
+extern "C" AcResult
+acDeviceLoadIntUniform(const Device d, const Stream stream, const AcIntParam param,
+                       const int value)
+{
+    (void)stream;
+    if (!d || (int)param < 0 || param >= NUM_INT_PARAMS)
+        return AC_FAILURE;
+    AcMeshInfo info        = d->config;
+    info.int_params[param] = value;
+    const AcResult r       = refresh_config(d, info);
+    if (r == AC_SUCCESS)
+        d->solve_variant = d->config.int_params[AC_debug_plain_kernel] ? 0 : 1;
+    return r;
+}
+
+extern "C" AcResult
+acDeviceStoreScalarUniform(const Device d, const Stream stream, const AcRealParam param,
+                           AcReal* value)
+{
+    (void)stream;
+    if (!d || !value || (int)param < 0 || param >= NUM_REAL_PARAMS)
+        return AC_FAILURE;
+    *value = d->config.real_params[param];
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceLoadMeshInfo(const Device d, const AcMeshInfo config)
+{
+    if (!d)
+        return AC_FAILURE;
+    return refresh_config(d, config);
+}
+
+extern "C" AcMeshInfo
+acDeviceGetConfig(const Device d)
+{
+    AcMeshInfo info;
+    if (!d) {
+        memset(&info, 0, sizeof(info));
+        return info;
+    }
+    return d->config;
+}
+
+/* ---- host <-> device ---- */
+
+static bool
+host_matches(const Device d, const AcMeshInfo& host)
+{
+    AcMeshInfo h = host;
+    if (acHostUpdateParams(&h) != AC_SUCCESS)
+        return false;
+    const int3 m = h.int3_params[AC_mlocal];
+    return m.x == d->geom.mx && m.y == d->geom.my && m.z == d->geom.mz;
+}
+
+extern "C" AcResult
+acDeviceLoadVertexBuffer(const Device d, const Stream stream, const AcMesh host_mesh,
+                         const VertexBufferHandle h)
+{
+    if (!d || !stream_ok(stream) || (int)h < 0 || h >= NUM_VTXBUF_HANDLES)
+        return AC_FAILURE;
+    if (!host_mesh.vertex_buffer[h])
+        return AC_NOT_ALLOCATED;
+    if (!host_matches(d, host_mesh.info)) {
+        fprintf(stderr, "astaroth_b200: host mesh dimensions differ from the device's\n");
+        return AC_FAILURE;
+    }
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    AC_CUDA_CHECK(cudaMemcpyAsync(d->f.in[h], host_mesh.vertex_buffer[h],
+                                  (size_t)d->geom.cells * sizeof(double),
+                                  cudaMemcpyHostToDevice, d->streams[stream]));
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceLoadMesh(const Device d, const Stream stream, const AcMesh host_mesh)
+{
+    int res = 0;
+    for (int q = 0; q < AC_NF; ++q)
+        res |= acDeviceLoadVertexBuffer(d, stream, host_mesh, (VertexBufferHandle)q);
+    return (AcResult)res;
+}
+
+extern "C" AcResult
+acDeviceStoreVertexBuffer(const Device d, const Stream stream, const VertexBufferHandle h,
+                          AcMesh* host_mesh)
+{
+    if (!d || !host_mesh || !stream_ok(stream) || (int)h < 0 || h >= NUM_VTXBUF_HANDLES)
+        return AC_FAILURE;
+    if (!host_mesh->vertex_buffer[h])
+        return AC_NOT_ALLOCATED;
+    if (!host_matches(d, host_mesh->info)) {
+        fprintf(stderr, "astaroth_b200: host mesh dimensions differ from the device's\n");
+        return AC_FAILURE;
+    }
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    AC_CUDA_CHECK(cudaMemcpyAsync(host_mesh->vertex_buffer[h], d->f.in[h],
+                                  (size_t)d->geom.cells * sizeof(double),
+                                  cudaMemcpyDeviceToHost, d->streams[stream]));
+    /* The host array is ready when the call returns. */
+    AC_CUDA_CHECK(cudaStreamSynchronize(d->streams[stream]));
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceStoreMesh(const Device d, const Stream stream, AcMesh* host_mesh)
+{
+    int res = 0;
+    for (int q = 0; q < AC_NF; ++q)
+        res |= acDeviceStoreVertexBuffer(d, stream, (VertexBufferHandle)q, host_mesh);
+    return (AcResult)res;
+}
+
+extern "C" AcResult
+acDeviceSetVertexBuffer(const Device d, const Stream stream, const VertexBufferHandle h,
+                        const AcReal value)
+{
+    if (!d || !stream_ok(stream) || (int)h < 0 || h >= NUM_VTXBUF_HANDLES)
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    AC_CUDA_CHECK(ac_launch_fill(d->f.in[h], d->geom.cells, value, d->streams[stream],
+                                 &d->launches));
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceFlushOutputBuffers(const Device d, const Stream stream)
+{
+    if (!d || !stream_ok(stream))
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    for (int q = 0; q < AC_NF; ++q)
+        AC_CUDA_CHECK(cudaMemsetAsync(d->f.out[q], 0, (size_t)d->geom.cells * sizeof(double),
+                                      d->streams[stream]));
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceResetMesh(const Device d, const Stream stream)
+{
+    if (!d || !stream_ok(stream))
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    for (int q = 0; q < AC_NF; ++q) {
+        AC_CUDA_CHECK(cudaMemsetAsync(d->f.in[q], 0, (size_t)d->geom.cells * sizeof(double),
+                                      d->streams[stream]));
+        AC_CUDA_CHECK(cudaMemsetAsync(d->f.out[q], 0, (size_t)d->geom.cells * sizeof(double),
+                                      d->streams[stream]));
+    }
+    return AC_SUCCESS;
+}
+
+/* ---- integration ---- */
+
+static bool
+is_whole_interior(const Device d, const Volume start, const Volume end)
+{
+    return start.x == NGHOST && start.y == NGHOST && start.z == NGHOST &&
+           end.x == (size_t)(d->geom.nx + NGHOST) && end.y == (size_t)(d->geom.ny + NGHOST) &&
+           end.z == (size_t)(d->geom.nz + NGHOST);
+}
+
+static RkCoef
+rk_coef(const int step, const double dt)
+{
+    /* Williamson 2N RK3, acc-runtime/stdlib/integrators.h:11-13 */
+    const double alpha[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
+    const double beta[3]  = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
+    RkCoef rk;
+    rk.step = step;
+    rk.dt   = dt;
+    rk.beta = beta[step];
+    rk.ab   = step == 0 ? 0.0 : alpha[step] / beta[step - 1];
+    return rk;
+}
+
+static cudaError_t
+launch_substep(Device d, cudaStream_t st, const int step, const double dt,
+               unsigned long long* launches)
+{
+    StencilCoef sc;
+    PhysConst pc;
+    ac_make_stencil(d->config, &sc);
+    ac_make_phys(d->config, &pc);
+    return ac_launch_solve64(d->geom, d->f, sc, pc, rk_coef(step, dt), d->solve_variant, st,
+                             launches);
+}
+
+extern "C" AcResult
+acDeviceIntegrateSubstep(const Device d, const Stream stream, const int step_number,
+                         const Volume start, const Volume end, const AcReal dt)
+{
+    if (!d || !stream_ok(stream) || step_number < 0 || step_number > 2)
+        return AC_FAILURE;
+    /* As the reference's default (two-pass) build, device.cc:965-970, only the
+     * whole interior is accepted. */
+    if (!is_whole_interior(d, start, end)) {
+        fprintf(stderr, "astaroth_b200: acDeviceIntegrateSubstep needs start = nmin and "
+                        "end = nmin + nlocal\n");
+        return AC_FAILURE;
+    }
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    AC_CUDA_CHECK(launch_substep(d, d->streams[stream], step_number, dt, &d->launches));
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDevicePeriodicBoundcondStep(const Device d, const Stream stream, const VertexBufferHandle h,
+                              const Volume start, const Volume end)
+{
+    if (!d || !stream_ok(stream) || (int)h < 0 || h >= NUM_VTXBUF_HANDLES)
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    double* p[1] = {d->f.in[h]};
+    AC_CUDA_CHECK(ac_launch_periodic(d->geom, p, 1, start, end, d->streams[stream],
+                                     &d->launches));
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDevicePeriodicBoundconds(const Device d, const Stream stream, const Volume start,
+                           const Volume end)
+{
+    if (!d || !stream_ok(stream))
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    AC_CUDA_CHECK(ac_launch_periodic(d->geom, d->f.in, AC_NF, start, end, d->streams[stream],
+                                     &d->launches));
+    return AC_SUCCESS;
+}
+
+static cudaError_t
+record_step(Device d, cudaStream_t st, const double dt, unsigned long long* launches)
+{
+    const Volume m0 = {0, 0, 0};
+    const Volume m1 = {(size_t)d->geom.mx, (size_t)d->geom.my, (size_t)d->geom.mz};
+    for (int s = 0; s < 3; ++s) {
+        cudaError_t e = ac_launch_periodic(d->geom, d->f.in, AC_NF, m0, m1, st, launches);
+        if (e != cudaSuccess)
+            return e;
+        e = launch_substep(d, st, s, dt, launches);
+        if (e != cudaSuccess)
+            return e;
+        acDeviceSwapBuffers(d);
+    }
+    return cudaSuccess;
+}
+
+extern "C" AcResult
+acDeviceIntegrateStep(const Device d, const Stream stream, const AcReal dt)
+{
+    if (!d || !stream_ok(stream))
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    cudaStream_t st = d->streams[stream];
+    /* All fields must be in the same buffer for the graph (true unless the
+     * caller swapped single fields); otherwise run the launches directly. */
+    int parity = d->f.in[0] == d->in_block ? 0 : 1;
+    for (int q = 1; q < AC_NF; ++q)
+        if ((d->f.in[q] == d->in_block + (size_t)q * d->geom.cells ? 0 : 1) != parity)
+            parity = -1;
+    if (parity < 0) {
+        AC_CUDA_CHECK(record_step(d, st, dt, &d->launches));
+        return AC_SUCCESS;
+    }
+    StepGraph& sg = d->graphs[stream][parity];
+    if (!sg.valid || sg.dt != dt) {
+        if (sg.valid)
+            cudaGraphExecDestroy(sg.exec);
+        sg.valid = 0;
+        cudaGraph_t graph;
+        AC_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t rec = record_step(d, st, dt, NULL);
+        const cudaError_t end = cudaStreamEndCapture(st, &graph);
+        acDeviceSwapBuffers(d); /* undo the capture's swaps (three swaps = one) */
+        AC_CUDA_CHECK(rec);
+        AC_CUDA_CHECK(end);
+        const cudaError_t inst = cudaGraphInstantiate(&sg.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        AC_CUDA_CHECK(inst);
+        sg.valid = 1;
+        sg.dt    = dt;
+    }
+    AC_CUDA_CHECK(cudaGraphLaunch(sg.exec, st));
+    d->launches += 6;
+    acDeviceSwapBuffers(d);
+    return AC_SUCCESS;
+}
+
+/* ---- reductions ---- */
+
+static AcResult
+reduce_common(const Device d, const Stream stream, const AcReduction r, const int kind,
+              const VertexBufferHandle* h, AcReal* result)
+{
+    if (!d || !result || !stream_ok(stream))
+        return AC_FAILURE;
+    for (int q = 0; q < kind; ++q)
+        if ((int)h[q] < 0 || h[q] >= NUM_VTXBUF_HANDLES)
+            return AC_NOT_ALLOCATED;
+    const int map = kind == 1 ? r.map_vtxbuf_single
+                              : kind == 3 ? r.map_vtxbuf_vec : r.map_vtxbuf_vec_scal;
+    const bool map_ok = kind == 1 ? (map >= AC_MAP_VTXBUF && map <= AC_MAP_VTXBUF_EXP_SQUARE)
+                        : kind == 3 ? (map >= AC_MAP_VTXBUF3_NORM &&
+                                       map <= AC_MAP_VTXBUF3_EXP_SQUARE)
+                                    : (map >= AC_MAP_VTXBUF4_ALFVEN_NORM &&
+                                       map <= AC_MAP_VTXBUF4_ALFVEN_SQUARE);
+    if (!map_ok) {
+        fprintf(stderr, "astaroth_b200: invalid reduction type for this call\n");
+        return AC_FAILURE;
+    }
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    /* Reductions observe all previously issued work of this device
+     * (the reference synchronizes the device first, reductions.cu:103). */
+    for (int s = 0; s < NUM_STREAMS; ++s)
+        if (s != (int)stream)
+            AC_CUDA_CHECK(cudaStreamSynchronize(d->streams[s]));
+    const double* fp[4];
+    for (int q = 0; q < kind; ++q)
+        fp[q] = d->f.in[h[q]];
+    cudaStream_t st = d->streams[stream];
+    AC_CUDA_CHECK(ac_launch_reduce(d->geom, fp, kind, map, r.reduce_op, d->red, st,
+                                   &d->launches));
+    AC_CUDA_CHECK(cudaMemcpyAsync(d->host_result, d->red.result, sizeof(double),
+                                  cudaMemcpyDeviceToHost, st));
+    AC_CUDA_CHECK(cudaStreamSynchronize(st));
+    *result = *d->host_result;
+    return AC_SUCCESS;
+}
+
+/* device.cc:1384-1401 */
+static AcReal
+post_process(const Device d, const AcReductionPostProcessingOp op, const AcReal v)
+{
+    if (op == AC_RMS) {
+        const AcReal inv_n =
+            AcReal(1.) / ((double)d->geom.nx * (double)d->geom.ny * (double)d->geom.nz);
+        return sqrt(inv_n * v);
+    }
+    return v;
+}
+
+extern "C" AcResult
+acDeviceReduceScalNoPostProcessing(const Device d, const Stream stream, const AcReduction r,
+                                   const VertexBufferHandle h, AcReal* result)
+{
+    return reduce_common(d, stream, r, 1, &h, result);
+}
+
+extern "C" AcResult
+acDeviceReduceScal(const Device d, const Stream stream, const AcReduction r,
+                   const VertexBufferHandle h, AcReal* result)
+{
+    const AcResult res = reduce_common(d, stream, r, 1, &h, result);
+    if (res == AC_SUCCESS)
+        *result = post_process(d, r.post_processing_op, *result);
+    return res;
+}
+
+extern "C" AcResult
+acDeviceReduceVecNoPostProcessing(const Device d, const Stream stream, const AcReduction r,
+                                  const VertexBufferHandle a, const VertexBufferHandle b,
+                                  const VertexBufferHandle c, AcReal* result)
+{
+    const VertexBufferHandle h[3] = {a, b, c};
+    return reduce_common(d, stream, r, 3, h, result);
+}
+
+extern "C" AcResult
+acDeviceReduceVec(const Device d, const Stream stream, const AcReduction r,
+                  const VertexBufferHandle a, const VertexBufferHandle b,
+                  const VertexBufferHandle c, AcReal* result)
+{
+    const VertexBufferHandle h[3] = {a, b, c};
+    const AcResult res            = reduce_common(d, stream, r, 3, h, result);
+    if (res == AC_SUCCESS)
+        *result = post_process(d, r.post_processing_op, *result);
+    return res;
+}
+
+extern "C" AcResult
+acDeviceReduceVecScalNoPostProcessing(const Device d, const Stream stream, const AcReduction r,
+                                      const VertexBufferHandle a, const VertexBufferHandle b,
+                                      const VertexBufferHandle c, const VertexBufferHandle e,
+                                      AcReal* result)
+{
+    const VertexBufferHandle h[4] = {a, b, c, e};
+    return reduce_common(d, stream, r, 4, h, result);
+}
+
+extern "C" AcResult
+acDeviceReduceVecScal(const Device d, const Stream stream, const AcReduction r,
+                      const VertexBufferHandle a, const VertexBufferHandle b,
+                      const VertexBufferHandle c, const VertexBufferHandle e, AcReal* result)
+{
+    const VertexBufferHandle h[4] = {a, b, c, e};
+    const AcResult res            = reduce_common(d, stream, r, 4, h, result);
+    if (res == AC_SUCCESS)
+        *result = post_process(d, r.post_processing_op, *result);
+    return res;
+}
+
+/* ---- misc ---- */
+
+extern "C" AcResult
+acDeviceGetVertexBufferPtrs(Device d, const VertexBufferHandle h, AcReal** in, AcReal** out)
+{
+    if (!d || !in || !out || (int)h < 0 || h >= NUM_VTXBUF_HANDLES)
+        return AC_FAILURE;
+    *in  = d->f.in[h];
+    *out = d->f.out[h];
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceMemGetInfo(const Device d, size_t* free_mem, size_t* total_mem)
+{
+    if (!d || !free_mem || !total_mem)
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    AC_CUDA_CHECK(cudaMemGetInfo(free_mem, total_mem));
+    return AC_SUCCESS;
+}
+
+extern "C" void*
+acDeviceGetStreamHandle(const Device d, const Stream stream)
+{
+    if (!d || !stream_ok(stream))
+        return NULL;
+    return (void*)d->streams[stream];
+}
+
+extern "C" unsigned long long
+acDeviceGetLaunchCount(const Device d)
+{
+    return d ? d->launches : 0ull;
+}

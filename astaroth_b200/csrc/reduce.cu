@@ -1,0 +1,228 @@
+/*
+ * Scalar / vector / vector+scalar reductions over the interior, fused in one
+ * launch: map -> per-thread accumulate -> warp shuffle -> block -> one atomic
+ * ticket per block; the last block to finish combines the per-block partials
+ * in a fixed order and writes the single result.
+ *
+ * Reference: acKernelReduceScal/Vec/VecScal, src/core/kernels/reductions.cu:95-170
+ * (a map kernel writing an N^3 scratch array, then cub::DeviceReduce), map
+ * kernels acc-runtime/stdlib/map.h:29-150, reduction types stdlib/reduction.h:1-8.
+ * Here the map never goes through memory and the traffic is one read of the
+ * fields.  Sums are accumulated as double-double (error-free two-sum), so the
+ * result is the correctly rounded sum up to the map's own rounding; the
+ * order is fixed by the grid, so repeated calls give identical bits.
+ */
+#include "internal.h"
+
+namespace {
+
+constexpr int kTpb = 256;
+
+struct DD {
+    double hi, lo;
+};
+
+__device__ __forceinline__ DD
+dd_add(const DD x, const double y)
+{
+    const double s  = x.hi + y;
+    const double bb = s - x.hi;
+    double e        = (x.hi - (s - bb)) + (y - bb);
+    e += x.lo;
+    const double hi = s + e;
+    return DD{hi, e - (hi - s)};
+}
+
+__device__ __forceinline__ DD
+dd_add(const DD x, const DD y)
+{
+    const double s  = x.hi + y.hi;
+    const double bb = s - x.hi;
+    double e        = (x.hi - (s - bb)) + (y.hi - bb);
+    e += x.lo + y.lo;
+    const double hi = s + e;
+    return DD{hi, e - (hi - s)};
+}
+
+struct ReduceFields {
+    const double* p[4];
+};
+
+__device__ __forceinline__ double
+map_value(const int map, const ReduceFields& f, const long long idx)
+{
+    const double a = f.p[0][idx];
+    switch (map) {
+    case AC_MAP_VTXBUF:
+        return a;
+    case AC_MAP_VTXBUF_SQUARE:
+        return a * a;
+    case AC_MAP_VTXBUF_EXP_SQUARE: {
+        const double e = exp(a);
+        return e * e;
+    }
+    default:
+        break;
+    }
+    const double b  = f.p[1][idx];
+    const double c  = f.p[2][idx];
+    const double sq = a * a + b * b + c * c;
+    switch (map) {
+    case AC_MAP_VTXBUF3_NORM:
+        return sqrt(sq);
+    case AC_MAP_VTXBUF3_SQUARE:
+        return sq;
+    case AC_MAP_VTXBUF3_EXP_SQUARE: {
+        const double ea = exp(a), eb = exp(b), ec = exp(c);
+        return ea * ea + eb * eb + ec * ec;
+    }
+    case AC_MAP_VTXBUF4_ALFVEN_NORM:
+        return sqrt(sq) / sqrt(exp(f.p[3][idx]));
+    case AC_MAP_VTXBUF4_ALFVEN_SQUARE:
+        return sq / exp(f.p[3][idx]);
+    default:
+        return 0;
+    }
+}
+
+__device__ __forceinline__ double
+combine(const int op, const double a, const double b)
+{
+    return op == AC_REDUCE_OP_MAX ? fmax(a, b) : fmin(a, b);
+}
+
+__global__ void __launch_bounds__(kTpb)
+reduce_kernel(const Geom g, const ReduceFields f, const int map, const int op,
+              double* __restrict__ partials, unsigned int* __restrict__ counter,
+              double* __restrict__ result)
+{
+    __shared__ double s_hi[kTpb / 32];
+    __shared__ double s_lo[kTpb / 32];
+    __shared__ bool s_last;
+    const bool is_sum  = op == AC_REDUCE_OP_SUM;
+    const double ident = op == AC_REDUCE_OP_MAX ? -INFINITY : INFINITY;
+
+    DD acc{0.0, 0.0};
+    double ext          = ident;
+    const long long rows = (long long)g.ny * g.nz;
+    for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+        const int j          = (int)(r % g.ny);
+        const int k          = (int)(r / g.ny);
+        const long long base = NGHOST + (long long)(j + NGHOST) * g.mx +
+                               (long long)(k + NGHOST) * g.mxy;
+        for (int i = threadIdx.x; i < g.nx; i += kTpb) {
+            const double v = map_value(map, f, base + i);
+            if (is_sum)
+                acc = dd_add(acc, v);
+            else
+                ext = combine(op, ext, v);
+        }
+    }
+    /* warp */
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        if (is_sum) {
+            DD other{__shfl_xor_sync(0xffffffffu, acc.hi, o),
+                     __shfl_xor_sync(0xffffffffu, acc.lo, o)};
+            acc = dd_add(acc, other);
+        }
+        else {
+            ext = combine(op, ext, __shfl_xor_sync(0xffffffffu, ext, o));
+        }
+    }
+    if (lane == 0) {
+        s_hi[warp] = is_sum ? acc.hi : ext;
+        s_lo[warp] = is_sum ? acc.lo : 0.0;
+    }
+    __syncthreads();
+    /* block */
+    if (threadIdx.x == 0) {
+        DD b{0.0, 0.0};
+        double e = ident;
+        for (int w = 0; w < kTpb / 32; ++w) {
+            if (is_sum)
+                b = dd_add(b, DD{s_hi[w], s_lo[w]});
+            else
+                e = combine(op, e, s_hi[w]);
+        }
+        partials[2 * blockIdx.x]     = is_sum ? b.hi : e;
+        partials[2 * blockIdx.x + 1] = is_sum ? b.lo : 0.0;
+        __threadfence();
+        const unsigned int ticket = atomicAdd(counter, 1u);
+        s_last                    = ticket == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!s_last)
+        return;
+    /* last block: combine the partials in block order */
+    __threadfence();
+    DD t{0.0, 0.0};
+    double e = ident;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += kTpb) {
+        const volatile double* vp = partials;
+        if (is_sum)
+            t = dd_add(t, DD{vp[2 * b], vp[2 * b + 1]});
+        else
+            e = combine(op, e, vp[2 * b]);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        if (is_sum) {
+            DD other{__shfl_xor_sync(0xffffffffu, t.hi, o), __shfl_xor_sync(0xffffffffu, t.lo, o)};
+            t = dd_add(t, other);
+        }
+        else {
+            e = combine(op, e, __shfl_xor_sync(0xffffffffu, e, o));
+        }
+    }
+    if (lane == 0) {
+        s_hi[warp] = is_sum ? t.hi : e;
+        s_lo[warp] = is_sum ? t.lo : 0.0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        DD b{0.0, 0.0};
+        double x = ident;
+        for (int w = 0; w < kTpb / 32; ++w) {
+            if (is_sum)
+                b = dd_add(b, DD{s_hi[w], s_lo[w]});
+            else
+                x = combine(op, x, s_hi[w]);
+        }
+        *result  = is_sum ? b.hi + b.lo : x;
+        *counter = 0u;
+    }
+}
+
+} // namespace
+
+int
+ac_reduce_blocks(const Geom& g)
+{
+    const long long rows = (long long)g.ny * g.nz;
+    const long long cap  = 148LL * 8;
+    return (int)(rows < cap ? rows : cap);
+}
+
+cudaError_t
+ac_launch_reduce(const Geom& g, const double* const* fields, const int nfields, const int map,
+                 const int op, const ReduceScratch& scratch, cudaStream_t stream,
+                 unsigned long long* launches)
+{
+    if (nfields < 1 || nfields > 4)
+        return cudaErrorInvalidValue;
+    if (op != AC_REDUCE_OP_SUM && op != AC_REDUCE_OP_MAX && op != AC_REDUCE_OP_MIN)
+        return cudaErrorInvalidValue;
+    ReduceFields f;
+    for (int q = 0; q < 4; ++q)
+        f.p[q] = fields[q < nfields ? q : 0];
+    const int blocks = ac_reduce_blocks(g);
+    if (blocks > scratch.max_blocks)
+        return cudaErrorInvalidValue;
+    reduce_kernel<<<blocks, kTpb, 0, stream>>>(g, f, map, op, scratch.partials, scratch.counter,
+                                              scratch.result);
+    if (launches)
+        ++*launches;
+    return cudaGetLastError();
+}

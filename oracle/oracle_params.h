@@ -1,0 +1,21 @@
+/*
+ * Test infrastructure only (the oracle): the physics parameters passed to both
+ * CPU oracles (oracle/astaroth_oracle.c and the reference model built by
+ * oracle/ref_driver.cc).  The names are those of the reference's run_const
+ * params (acc-runtime/samples/mhd_modular/mhdsolver.ac:230-251).
+ */
+#pragma once
+
+typedef struct {
+    double ds[3];
+    double nu_visc;
+    double eta;
+    double cs_sound;
+    double gamma;
+    double cp_sound;
+    double lnrho0;
+    double lnT0;
+    double mu0;
+    double zeta;
+    double K_heatcond;
+} OracleParams;
