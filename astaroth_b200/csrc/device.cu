@@ -147,9 +147,12 @@ acDeviceCreate(const int id, const AcMeshInfo device_config, Device* device_hand
         return AC_FAILURE;
     }
 
-    device_s* d = (device_s*)calloc(1, sizeof(device_s));
+    /* CUtensorMap members need 64-byte alignment */
+    const size_t dbytes = (sizeof(device_s) + 63) / 64 * 64;
+    device_s* d         = (device_s*)aligned_alloc(64, dbytes);
     if (!d)
         return AC_FAILURE;
+    memset(d, 0, dbytes);
     d->id        = id;
     d->config    = info;
     d->geom      = ac_make_geom(info);
@@ -180,6 +183,7 @@ acDeviceCreate(const int id, const AcMeshInfo device_config, Device* device_hand
     CREATE_CHECK(cudaMemsetAsync(d->in_block, 0, bytes, d->streams[0]));
     CREATE_CHECK(cudaMemsetAsync(d->out_block, 0, bytes, d->streams[0]));
 
+    /* small scratch block: [partials 2*blocks][result 2][counter, err] */
     const int blocks    = ac_reduce_blocks(d->geom);
     d->red.max_blocks   = blocks;
     const size_t rbytes = (2 * (size_t)blocks + 2) * sizeof(double) + 64;
@@ -187,6 +191,11 @@ acDeviceCreate(const int id, const AcMeshInfo device_config, Device* device_hand
     CREATE_CHECK(cudaMemsetAsync(d->red.partials, 0, rbytes, d->streams[0]));
     d->red.result  = d->red.partials + 2 * (size_t)blocks;
     d->red.counter = (unsigned int*)(d->red.result + 2);
+    d->err_flag    = (int*)(d->red.counter + 4);
+    d->tmap_ok     = ac_make_tensor_map64(&d->tmap[0], d->in_block, d->geom) &&
+                 ac_make_tensor_map64(&d->tmap[1], d->out_block, d->geom);
+    if (d->tmap_ok)
+        CREATE_CHECK(ac_solve_tiled_init());
     CREATE_CHECK(cudaMallocHost((void**)&d->host_result, sizeof(double)));
     CREATE_CHECK(cudaStreamSynchronize(d->streams[0]));
 #undef CREATE_CHECK
@@ -221,6 +230,23 @@ acDevicePrintInfo(const Device d)
     return AC_SUCCESS;
 }
 
+/* Reads and clears the device error word (set by a kernel whose bounded wait
+ * on an mbarrier gave up); nonzero means the last results are invalid. */
+static AcResult
+check_device_error(const Device d, cudaStream_t st)
+{
+    int err = 0;
+    AC_CUDA_CHECK(cudaMemcpyAsync(&err, d->err_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+    AC_CUDA_CHECK(cudaStreamSynchronize(st));
+    if (err) {
+        fprintf(stderr, "astaroth_b200: a kernel timed out waiting for its TMA loads\n");
+        AC_CUDA_CHECK(cudaMemsetAsync(d->err_flag, 0, sizeof(int), st));
+        AC_CUDA_CHECK(cudaStreamSynchronize(st));
+        return AC_FAILURE;
+    }
+    return AC_SUCCESS;
+}
+
 extern "C" AcResult
 acDeviceSynchronizeStream(const Device d, const Stream stream)
 {
@@ -230,12 +256,12 @@ acDeviceSynchronizeStream(const Device d, const Stream stream)
     if (stream == STREAM_ALL) {
         for (int s = 0; s < NUM_STREAMS; ++s)
             AC_CUDA_CHECK(cudaStreamSynchronize(d->streams[s]));
-        return AC_SUCCESS;
+        return check_device_error(d, d->streams[0]);
     }
     if (!stream_ok(stream))
         return AC_FAILURE;
     AC_CUDA_CHECK(cudaStreamSynchronize(d->streams[stream]));
-    return AC_SUCCESS;
+    return check_device_error(d, d->streams[stream]);
 }
 
 extern "C" AcResult
@@ -483,6 +509,23 @@ rk_coef(const int step, const double dt)
     return rk;
 }
 
+/* Which buffer block holds every field's in-buffer: 0 = in_block, 1 = out_block,
+ * -1 = mixed (a single field was swapped on its own). */
+static int
+in_block_index(const Device d)
+{
+    int idx = -1;
+    for (int q = 0; q < AC_NF; ++q) {
+        const int b = d->f.in[q] == d->in_block + (size_t)q * d->geom.cells    ? 0
+                      : d->f.in[q] == d->out_block + (size_t)q * d->geom.cells ? 1
+                                                                                : -1;
+        if (b < 0 || (q > 0 && b != idx))
+            return -1;
+        idx = b;
+    }
+    return idx;
+}
+
 static cudaError_t
 launch_substep(Device d, cudaStream_t st, const int step, const double dt,
                unsigned long long* launches)
@@ -491,8 +534,11 @@ launch_substep(Device d, cudaStream_t st, const int step, const double dt,
     PhysConst pc;
     ac_make_stencil(d->config, &sc);
     ac_make_phys(d->config, &pc);
-    return ac_launch_solve64(d->geom, d->f, sc, pc, rk_coef(step, dt), d->solve_variant, st,
-                             launches);
+    const int blk = in_block_index(d);
+    if (d->solve_variant == 1 && d->tmap_ok && blk >= 0)
+        return ac_launch_solve64_tiled(d->geom, &d->tmap[blk], d->f, sc, pc, rk_coef(step, dt),
+                                       d->err_flag, st, launches);
+    return ac_launch_solve64(d->geom, d->f, sc, pc, rk_coef(step, dt), 0, st, launches);
 }
 
 extern "C" AcResult
@@ -564,10 +610,7 @@ acDeviceIntegrateStep(const Device d, const Stream stream, const AcReal dt)
     cudaStream_t st = d->streams[stream];
     /* All fields must be in the same buffer for the graph (true unless the
      * caller swapped single fields); otherwise run the launches directly. */
-    int parity = d->f.in[0] == d->in_block ? 0 : 1;
-    for (int q = 1; q < AC_NF; ++q)
-        if ((d->f.in[q] == d->in_block + (size_t)q * d->geom.cells ? 0 : 1) != parity)
-            parity = -1;
+    const int parity = in_block_index(d);
     if (parity < 0) {
         AC_CUDA_CHECK(record_step(d, st, dt, &d->launches));
         return AC_SUCCESS;

@@ -5,6 +5,7 @@
  */
 #pragma once
 
+#include <cuda.h> /* CUtensorMap (encoded through cudaGetDriverEntryPoint) */
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -86,6 +87,9 @@ struct StepGraph {
 };
 
 struct device_s {
+    CUtensorMap tmap[2]; /* 4-D (x, y, z, field) maps of in_block / out_block */
+    int tmap_ok;
+    int* err_flag;       /* device word set by kernels whose bounded waits gave up */
     int id;
     AcMeshInfo config;
     Geom geom;
@@ -120,6 +124,13 @@ cudaError_t ac_launch_reduce(const Geom& g, const double* const* fields, const i
                              cudaStream_t stream, unsigned long long* launches);
 
 int ac_reduce_blocks(const Geom& g);
+
+bool ac_tiled_supported(const Geom& g);
+cudaError_t ac_solve_tiled_init();
+bool ac_make_tensor_map64(void* map_out, double* base, const Geom& g);
+cudaError_t ac_launch_solve64_tiled(const Geom& g, const void* tmap_in, const Fields64& f,
+                                    const StencilCoef& sc, const PhysConst& pc, const RkCoef& rk,
+                                    int* err, cudaStream_t stream, unsigned long long* launches);
 
 /* Host-side setup helpers (device.cu). */
 void ac_make_stencil(const AcMeshInfo& info, StencilCoef* sc);

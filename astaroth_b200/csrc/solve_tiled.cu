@@ -1,0 +1,353 @@
+/*
+ * FP64 substep kernel, 2.5-D blocked (the production path on B200).
+ *
+ * Each CTA owns a 32 x 4 (x, y) tile of the interior and marches along z over
+ * a chunk of ZCHUNK planes.  A ring of RING = 8 shared-memory slots holds the
+ * planes z-3 .. z+3 the stencils of plane z need plus one plane in flight.
+ * One TMA instruction (cp.async.bulk.tensor.4d, no multicast) brings a whole
+ * plane of all 8 fields -- a (38 x 10 x 1 x 8) box of the in-buffer, halo
+ * included -- into a slot and signals an mbarrier; every cell value is read
+ * from HBM/L2 once per plane per CTA instead of once per stencil tap.
+ *
+ * The per-cell work (stencils, RHS, single-pass RK3 update) is the one of the
+ * plain kernel in solve.cu, reading taps from shared memory.  Reference:
+ * singlepass_solve / twopass_solve_intermediate,
+ * acc-runtime/samples/mhd_modular/mhdsolver.ac:524-612 (the reference issues
+ * every tap as a separate __ldg, acc-runtime/acc/stencilgen.c:2205).
+ *
+ * Waits on mbarriers are bounded: a wait that gives up sets *err and the
+ * kernel still runs to completion (all threads take the same path, so no
+ * __syncthreads is skipped); the host turns *err into AC_FAILURE.
+ */
+#include <cuda.h>
+
+#include "internal.h"
+#include "mhd_rhs.cuh"
+
+namespace {
+
+constexpr int TX    = 32;
+constexpr int TY    = 4;
+constexpr int HX    = TX + 2 * NGHOST;
+constexpr int HY    = TY + 2 * NGHOST;
+constexpr int PLANE = HX * HY;        /* doubles per field per plane */
+constexpr int SLOT  = AC_NF * PLANE;  /* doubles per ring slot */
+constexpr int RING  = 8;
+constexpr int ZCHUNK = 64;
+constexpr unsigned SLOT_BYTES = SLOT * sizeof(double);
+constexpr size_t SMEM_BYTES   = (size_t)RING * SLOT_BYTES + RING * sizeof(uint64_t);
+/* try_wait may suspend the thread for a short, implementation-defined time per
+ * call; 2^22 calls bound a wait to seconds even if a copy never lands. */
+constexpr long long kWaitLimit = 1LL << 22;
+
+__device__ __forceinline__ uint32_t
+smem_addr(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void
+mbar_init(uint64_t* bar, const unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
+                 : "memory");
+}
+
+__device__ __forceinline__ void
+fence_barrier_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void
+mbar_arrive_expect_tx(uint64_t* bar, const unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool
+mbar_try_wait(uint64_t* bar, const unsigned parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_addr(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool
+mbar_wait_bounded(uint64_t* bar, const unsigned parity)
+{
+    for (long long it = 0; it < kWaitLimit; ++it)
+        if (mbar_try_wait(bar, parity))
+            return true;
+    return false;
+}
+
+__device__ __forceinline__ void
+tma_load_plane(double* dst, const CUtensorMap* map, uint64_t* bar, const int x, const int y,
+               const int z)
+{
+    asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_addr(dst)),
+                 "l"(map), "r"(x), "r"(y), "r"(z), "r"(0), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+/* Taps of field q at offset (dx, dy, dz) from this thread's cell. */
+struct Taps {
+    const double* s;
+    int off[7]; /* per dz = -3..3: slot base + this thread's (x, y) position */
+    __device__ __forceinline__ double operator()(const int q, const int dx, const int dy,
+                                                 const int dz) const
+    {
+        return s[off[dz + 3] + q * PLANE + dy * HX + dx];
+    }
+};
+
+template <int A>
+__device__ __forceinline__ double
+tap1(const Taps& t, const int q, const int k)
+{
+    return A == 0 ? t(q, k, 0, 0) : A == 1 ? t(q, 0, k, 0) : t(q, 0, 0, k);
+}
+
+template <int A>
+__device__ __forceinline__ double
+d1(const Taps& t, const int q, const double* c)
+{
+    double r = c[0] * (tap1<A>(t, q, 1) - tap1<A>(t, q, -1));
+    r        = fma(c[1], tap1<A>(t, q, 2) - tap1<A>(t, q, -2), r);
+    r        = fma(c[2], tap1<A>(t, q, 3) - tap1<A>(t, q, -3), r);
+    return r;
+}
+
+template <int A>
+__device__ __forceinline__ double
+d2_sides(const Taps& t, const int q, const double* d)
+{
+    double r = d[1] * (tap1<A>(t, q, 1) + tap1<A>(t, q, -1));
+    r        = fma(d[2], tap1<A>(t, q, 2) + tap1<A>(t, q, -2), r);
+    r        = fma(d[3], tap1<A>(t, q, 3) + tap1<A>(t, q, -3), r);
+    return r;
+}
+
+/* tap at +a along axis A and +b along axis B (A < B) */
+template <int A, int B>
+__device__ __forceinline__ double
+tap2(const Taps& t, const int q, const int a, const int b)
+{
+    if (A == 0 && B == 1)
+        return t(q, a, b, 0);
+    if (A == 0 && B == 2)
+        return t(q, a, 0, b);
+    return t(q, 0, a, b);
+}
+
+template <int A, int B>
+__device__ __forceinline__ double
+dmix(const Taps& t, const int q, const double* e)
+{
+    double r = 0;
+#pragma unroll
+    for (int k = 1; k <= 3; ++k) {
+        const double s = (tap2<A, B>(t, q, k, k) + tap2<A, B>(t, q, -k, -k)) -
+                         (tap2<A, B>(t, q, k, -k) + tap2<A, B>(t, q, -k, k));
+        r = k == 1 ? e[0] * s : fma(e[k - 1], s, r);
+    }
+    return r;
+}
+
+__device__ __forceinline__ void
+scal_derivs(const Taps& t, const int q, const StencilCoef& sc, ScalD<double>& o)
+{
+    o.v    = t(q, 0, 0, 0);
+    o.g[0] = d1<0>(t, q, sc.d1[0]);
+    o.g[1] = d1<1>(t, q, sc.d1[1]);
+    o.g[2] = d1<2>(t, q, sc.d1[2]);
+    o.lap  = (sc.d2[0][0] + sc.d2[1][0] + sc.d2[2][0]) * o.v + d2_sides<0>(t, q, sc.d2[0]) +
+            d2_sides<1>(t, q, sc.d2[1]) + d2_sides<2>(t, q, sc.d2[2]);
+}
+
+__device__ __forceinline__ void
+vec_derivs(const Taps& t, const int q0, const StencilCoef& sc, VecD<double>& o)
+{
+    double diag[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const int q = q0 + c;
+        o.v[c]      = t(q, 0, 0, 0);
+        o.g[c][0]   = d1<0>(t, q, sc.d1[0]);
+        o.g[c][1]   = d1<1>(t, q, sc.d1[1]);
+        o.g[c][2]   = d1<2>(t, q, sc.d1[2]);
+        const double s0 = d2_sides<0>(t, q, sc.d2[0]);
+        const double s1 = d2_sides<1>(t, q, sc.d2[1]);
+        const double s2 = d2_sides<2>(t, q, sc.d2[2]);
+        diag[c]  = sc.d2[c][0] * o.v[c] + (c == 0 ? s0 : c == 1 ? s1 : s2);
+        o.lap[c] = (sc.d2[0][0] + sc.d2[1][0] + sc.d2[2][0]) * o.v[c] + s0 + s1 + s2;
+    }
+    o.gd[0] = diag[0] + dmix<0, 1>(t, q0 + 1, sc.mix[0]) + dmix<0, 2>(t, q0 + 2, sc.mix[1]);
+    o.gd[1] = dmix<0, 1>(t, q0, sc.mix[0]) + diag[1] + dmix<1, 2>(t, q0 + 2, sc.mix[2]);
+    o.gd[2] = dmix<0, 2>(t, q0, sc.mix[1]) + dmix<1, 2>(t, q0 + 1, sc.mix[2]) + diag[2];
+}
+
+__global__ void __launch_bounds__(TX * TY, 1)
+solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const Fields64 f,
+                   const StencilCoef sc, const PhysConst pc, const RkCoef rk, int* err)
+{
+    extern __shared__ __align__(128) double smem[];
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)RING * SLOT);
+    const int lx = threadIdx.x, ly = threadIdx.y;
+    const int tid = ly * TX + lx;
+    const int x0  = blockIdx.x * TX;
+    const int y0  = blockIdx.y * TY;
+    const int z0  = blockIdx.z * ZCHUNK;
+    const int z1  = min(z0 + ZCHUNK, g.nz);
+    const int pfirst = z0 - NGHOST;    /* first plane needed (interior z index) */
+    const int plast  = z1 - 1 + NGHOST; /* last plane needed */
+
+    if (tid == 0) {
+        for (int s = 0; s < RING; ++s)
+            mbar_init(&bars[s], 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+        const int pend = min(plast, pfirst + RING - 1);
+        for (int p = pfirst; p <= pend; ++p) {
+            const int s = (p - pfirst) & (RING - 1);
+            mbar_arrive_expect_tx(&bars[s], SLOT_BYTES);
+            tma_load_plane(smem + (size_t)s * SLOT, &tmap, &bars[s], x0, y0, p + NGHOST);
+        }
+    }
+
+    const int x = x0 + lx, y = y0 + ly;
+    const bool active = x < g.nx && y < g.ny;
+    const PhysT<double> p = phys_cast<double>(pc);
+    const int cell_off    = (ly + NGHOST) * HX + (lx + NGHOST);
+    bool ok               = true;
+    int waited            = pfirst - 1;
+
+    for (int z = z0; z < z1; ++z) {
+        for (int q = waited + 1; q <= z + NGHOST; ++q) {
+            const int s = (q - pfirst) & (RING - 1);
+            /* after one failed wait the kernel stops waiting and only runs out */
+            if (ok)
+                ok = mbar_wait_bounded(&bars[s], (unsigned)(((q - pfirst) / RING) & 1));
+        }
+        waited = z + NGHOST;
+
+        Taps t;
+        t.s = smem;
+#pragma unroll
+        for (int k = 0; k < 7; ++k)
+            t.off[k] = ((z - NGHOST + k - pfirst) & (RING - 1)) * SLOT + cell_off;
+
+        if (active) {
+            ScalD<double> L, S;
+            VecD<double> U, A;
+            scal_derivs(t, VTXBUF_LNRHO, sc, L);
+            scal_derivs(t, VTXBUF_ENTROPY, sc, S);
+            vec_derivs(t, VTXBUF_UUX, sc, U);
+            vec_derivs(t, VTXBUF_AX, sc, A);
+            double r[AC_NF];
+            mhd_rates(L, S, U, A, p, r);
+            const double val[AC_NF] = {L.v, U.v[0], U.v[1], U.v[2], A.v[0], A.v[1], A.v[2], S.v};
+            const long long idx = (long long)(x + NGHOST) + (long long)(y + NGHOST) * g.mx +
+                                  (long long)(z + NGHOST) * g.mxy;
+#pragma unroll
+            for (int qf = 0; qf < AC_NF; ++qf) {
+                double upd = rk.dt * r[qf];
+                if (rk.step > 0)
+                    upd = fma(rk.ab, val[qf] - f.out[qf][idx], upd);
+                f.out[qf][idx] = fma(rk.beta, upd, val[qf]);
+            }
+        }
+        __syncthreads(); /* every thread is done with plane z - 3 */
+        const int next = z - NGHOST + RING;
+        if (tid == 0 && next <= plast) {
+            const int s = (next - pfirst) & (RING - 1);
+            mbar_arrive_expect_tx(&bars[s], SLOT_BYTES);
+            tma_load_plane(smem + (size_t)s * SLOT, &tmap, &bars[s], x0, y0, next + NGHOST);
+        }
+    }
+    if (!ok)
+        atomicExch(err, 1);
+}
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn
+encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+} // namespace
+
+bool
+ac_tiled_supported(const Geom& g)
+{
+    /* TMA: global strides must be multiples of 16 bytes (mx even) and the box
+     * must not exceed the tensor (nx >= 32, ny >= 4). */
+    return (g.mx % 2) == 0 && g.nx >= TX && g.ny >= TY;
+}
+
+bool
+ac_make_tensor_map64(void* map_out, double* base, const Geom& g)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn || !ac_tiled_supported(g))
+        return false;
+    const cuuint64_t dims[4]    = {(cuuint64_t)g.mx, (cuuint64_t)g.my, (cuuint64_t)g.mz,
+                                   (cuuint64_t)AC_NF};
+    const cuuint64_t strides[3] = {(cuuint64_t)g.mx * 8, (cuuint64_t)g.mxy * 8,
+                                   (cuuint64_t)g.cells * 8};
+    const cuuint32_t box[4]     = {HX, HY, 1, AC_NF};
+    const cuuint32_t estr[4]    = {1, 1, 1, 1};
+    const CUresult r = fn((CUtensorMap*)map_out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims,
+                          strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+/* Opts the kernel in to its dynamic shared memory on the current device; called
+ * by acDeviceCreate, outside any stream capture. */
+cudaError_t
+ac_solve_tiled_init()
+{
+    return cudaFuncSetAttribute(solve_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)SMEM_BYTES);
+}
+
+cudaError_t
+ac_launch_solve64_tiled(const Geom& g, const void* tmap_in, const Fields64& f,
+                        const StencilCoef& sc, const PhysConst& pc, const RkCoef& rk, int* err,
+                        cudaStream_t stream, unsigned long long* launches)
+{
+    const dim3 tpb(TX, TY, 1);
+    const dim3 bpg((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + ZCHUNK - 1) / ZCHUNK);
+    solve_tiled_kernel<<<bpg, tpb, SMEM_BYTES, stream>>>(*(const CUtensorMap*)tmap_in, g, f, sc,
+                                                         pc, rk, err);
+    if (launches)
+        ++*launches;
+    return cudaGetLastError();
+}

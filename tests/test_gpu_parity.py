@@ -299,6 +299,8 @@ def test_api_errors_and_state():
         assert lib.acDeviceSwapBuffer(dev.handle, 3) == 0
         out = dev.store_mesh()
         assert np.array_equal(out[2], f[2]) and not out[3].any()
+        dev.periodic_boundconds()
+        dev.synchronize()
         assert dev.launch_count() > 0
     assert lib.acDeviceSynchronizeStream(None, 0) == 1
 
