@@ -84,88 +84,164 @@ ac_rcp(const float x)
     return __frcp_rn(x);
 }
 
+/* The RHS is evaluated in two halves so that two warp groups can share one
+ * cell: the hydro half owns lnrho and uu (continuity, momentum), the magnetic
+ * half owns aa and entropy (induction, entropy).  Each half first prepares
+ * the values the other needs, the two exchange them, then each finishes its
+ * four rates.  mhd_rates() runs both halves in one thread, so split and
+ * unsplit kernels evaluate the same expressions. */
+/* Exchange records as flat arrays (registers, and one shared-memory row per
+ * entry when two warp groups share a cell). */
+enum {
+    H2M_U   = 0, /* u[3] */
+    H2M_GL  = 3, /* grad lnrho[3] */
+    H2M_LAPL = 6,
+    H2M_SS   = 7, /* S:S */
+    H2M_DIVU = 8,
+    H2M_E    = 9, /* exp(gamma s/cp + (gamma-1)(lnrho - lnrho0)) */
+    H2M_INV_RHO = 10, /* exp(-lnrho) */
+    AC_H2M_COUNT = 11
+};
+enum {
+    M2H_GS = 0, /* grad s[3] */
+    M2H_J  = 3, /* current density[3] */
+    M2H_B  = 6, /* magnetic field[3] */
+    AC_M2H_COUNT = 9
+};
+
+template <typename T>
+struct HydroToMag {
+    T a[AC_H2M_COUNT];
+};
+
+template <typename T>
+struct MagToHydro {
+    T a[AC_M2H_COUNT];
+};
+
+template <typename T>
+struct Strain {
+    T S00, S11, S22, S01, S02, S12;
+};
+
+template <typename T>
+__device__ __forceinline__ void
+hydro_prepare(const ScalD<T>& L, const T s_value, const VecD<T>& U, const PhysT<T>& p,
+              HydroToMag<T>& x, Strain<T>& S)
+{
+    const T third     = (T)(1.0 / 3.0);
+    x.a[H2M_DIVU]     = U.g[0][0] + U.g[1][1] + U.g[2][2];
+    S.S00 = (T)(2.0 / 3.0) * U.g[0][0] - third * (U.g[1][1] + U.g[2][2]);
+    S.S11 = (T)(2.0 / 3.0) * U.g[1][1] - third * (U.g[0][0] + U.g[2][2]);
+    S.S22 = (T)(2.0 / 3.0) * U.g[2][2] - third * (U.g[0][0] + U.g[1][1]);
+    S.S01 = (T)0.5 * (U.g[0][1] + U.g[1][0]);
+    S.S02 = (T)0.5 * (U.g[0][2] + U.g[2][0]);
+    S.S12 = (T)0.5 * (U.g[1][2] + U.g[2][1]);
+    x.a[H2M_SS] = S.S00 * S.S00 + S.S11 * S.S11 + S.S22 * S.S22 +
+                  (T)2 * (S.S01 * S.S01 + S.S02 * S.S02 + S.S12 * S.S12);
+    const T arg      = p.gamma_inv_cp * s_value + p.gamma_m1 * (L.v - p.lnrho0);
+    x.a[H2M_E]       = ac_exp(arg);
+    x.a[H2M_INV_RHO] = ac_exp(-L.v);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        x.a[H2M_U + a]  = U.v[a];
+        x.a[H2M_GL + a] = L.g[a];
+    }
+    x.a[H2M_LAPL] = L.lap;
+}
+
+template <typename T>
+__device__ __forceinline__ void
+mag_prepare(const ScalD<T>& Sg, const VecD<T>& A, const PhysT<T>& p, MagToHydro<T>& m)
+{
+    m.a[M2H_B + 0] = A.g[2][1] - A.g[1][2];
+    m.a[M2H_B + 1] = A.g[0][2] - A.g[2][0];
+    m.a[M2H_B + 2] = A.g[1][0] - A.g[0][1];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        m.a[M2H_J + a]  = (A.gd[a] - A.lap[a]) * p.inv_mu0;
+        m.a[M2H_GS + a] = Sg.g[a];
+    }
+}
+
+/* r[0] = dlnrho/dt, r[1..3] = du/dt */
+template <typename T>
+__device__ __forceinline__ void
+hydro_rates(const ScalD<T>& L, const VecD<T>& U, const Strain<T>& S, const HydroToMag<T>& x,
+            const MagToHydro<T>& m, const PhysT<T>& p, T r[4])
+{
+    const T ux = U.v[0], uy = U.v[1], uz = U.v[2];
+    r[0]        = -(ux * L.g[0] + uy * L.g[1] + uz * L.g[2]) - x.a[H2M_DIVU];
+    const T cs2 = p.cs2_sound * x.a[H2M_E];
+    const T* j  = &m.a[M2H_J];
+    const T* B  = &m.a[M2H_B];
+    const T jxB[3] = {j[1] * B[2] - j[2] * B[1], j[2] * B[0] - j[0] * B[2],
+                      j[0] * B[1] - j[1] * B[0]};
+    const T SL[3]  = {S.S00 * L.g[0] + S.S01 * L.g[1] + S.S02 * L.g[2],
+                      S.S01 * L.g[0] + S.S11 * L.g[1] + S.S12 * L.g[2],
+                      S.S02 * L.g[0] + S.S12 * L.g[1] + S.S22 * L.g[2]};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const T adv = U.g[c][0] * ux + U.g[c][1] * uy + U.g[c][2] * uz;
+        const T pg  = p.inv_cp * m.a[M2H_GS + c] + L.g[c];
+        r[1 + c]    = -adv - cs2 * pg + x.a[H2M_INV_RHO] * jxB[c] +
+                   p.nu * (U.lap[c] + (T)2 * SL[c]) + p.visc_gd * U.gd[c];
+    }
+}
+
+/* r[0..2] = dA/dt, r[3] = ds/dt */
+template <typename T>
+__device__ __forceinline__ void
+mag_rates(const ScalD<T>& Sg, const VecD<T>& A, const MagToHydro<T>& m, const HydroToMag<T>& x,
+          const PhysT<T>& p, T r[4])
+{
+    const T ux = x.a[H2M_U], uy = x.a[H2M_U + 1], uz = x.a[H2M_U + 2];
+    const T* B = &m.a[M2H_B];
+    const T* j = &m.a[M2H_J];
+    /* induction: u x B + eta lap A */
+    r[0] = (uy * B[2] - uz * B[1]) + p.eta * A.lap[0];
+    r[1] = (uz * B[0] - ux * B[2]) + p.eta * A.lap[1];
+    r[2] = (ux * B[1] - uy * B[0]) + p.eta * A.lap[2];
+    /* entropy: (rho T)^-1 (eta mu0 j.j + 2 rho nu S:S + zeta rho divu^2) + heat */
+    const T inv_rho = x.a[H2M_INV_RHO];
+    const T divu    = x.a[H2M_DIVU];
+    const T inv_T   = p.inv_exp_lnT0 * ac_rcp(x.a[H2M_E]);
+    const T jj      = j[0] * j[0] + j[1] * j[1] + j[2] * j[2];
+    const T heating = inv_T * (inv_rho * p.eta_mu0 * jj + (T)2 * p.nu * x.a[H2M_SS] +
+                               p.zeta * divu * divu);
+    /* heat conduction: K/rho (first + second.third); the reference's third term
+     * gamma (grad s/cp + grad lnrho) - grad lnrho equals its second term */
+    const T first = p.gamma_inv_cp * Sg.lap + p.gamma_m1 * x.a[H2M_LAPL];
+    T dot2        = 0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const T second = p.gamma_inv_cp * Sg.g[a] + p.gamma_m1 * x.a[H2M_GL + a];
+        dot2 += second * second;
+    }
+    const T heat = p.K * inv_rho * (first + dot2);
+    r[3]         = -(ux * Sg.g[0] + uy * Sg.g[1] + uz * Sg.g[2]) + heating + heat;
+}
+
 /* rates[8] in field order (lnrho, ux, uy, uz, ax, ay, az, entropy). */
 template <typename T>
 __device__ __forceinline__ void
 mhd_rates(const ScalD<T>& L, const ScalD<T>& Sg, const VecD<T>& U, const VecD<T>& A,
           const PhysT<T>& p, T r[AC_NF])
 {
-    const T ux = U.v[0], uy = U.v[1], uz = U.v[2];
-    const T divu = U.g[0][0] + U.g[1][1] + U.g[2][2];
-
-    /* continuity */
-    r[0] = -(ux * L.g[0] + uy * L.g[1] + uz * L.g[2]) - divu;
-
-    /* magnetic field and current */
-    const T Bx = A.g[2][1] - A.g[1][2];
-    const T By = A.g[0][2] - A.g[2][0];
-    const T Bz = A.g[1][0] - A.g[0][1];
-    const T jx = (A.gd[0] - A.lap[0]) * p.inv_mu0;
-    const T jy = (A.gd[1] - A.lap[1]) * p.inv_mu0;
-    const T jz = (A.gd[2] - A.lap[2]) * p.inv_mu0;
-
-    /* induction: u x B + eta lap A */
-    r[4] = (uy * Bz - uz * By) + p.eta * A.lap[0];
-    r[5] = (uz * Bx - ux * Bz) + p.eta * A.lap[1];
-    r[6] = (ux * By - uy * Bx) + p.eta * A.lap[2];
-
-    /* thermodynamics: E = exp(gamma s/cp + (gamma-1)(lnrho - lnrho0)) */
-    const T arg     = p.gamma_inv_cp * Sg.v + p.gamma_m1 * (L.v - p.lnrho0);
-    const T E       = ac_exp(arg);
-    const T cs2     = p.cs2_sound * E;
-    const T inv_rho = ac_exp(-L.v);
-    const T inv_T   = p.inv_exp_lnT0 * ac_rcp(E);
-
-    /* traceless rate of strain */
-    const T third = (T)(1.0 / 3.0);
-    const T S00   = (T)(2.0 / 3.0) * U.g[0][0] - third * (U.g[1][1] + U.g[2][2]);
-    const T S11   = (T)(2.0 / 3.0) * U.g[1][1] - third * (U.g[0][0] + U.g[2][2]);
-    const T S22   = (T)(2.0 / 3.0) * U.g[2][2] - third * (U.g[0][0] + U.g[1][1]);
-    const T S01   = (T)0.5 * (U.g[0][1] + U.g[1][0]);
-    const T S02   = (T)0.5 * (U.g[0][2] + U.g[2][0]);
-    const T S12   = (T)0.5 * (U.g[1][2] + U.g[2][1]);
-
-    /* momentum */
-    {
-        const T jxBx = jy * Bz - jz * By;
-        const T jxBy = jz * Bx - jx * Bz;
-        const T jxBz = jx * By - jy * Bx;
-        const T px   = p.inv_cp * Sg.g[0] + L.g[0];
-        const T py   = p.inv_cp * Sg.g[1] + L.g[1];
-        const T pz   = p.inv_cp * Sg.g[2] + L.g[2];
-        const T SLx  = S00 * L.g[0] + S01 * L.g[1] + S02 * L.g[2];
-        const T SLy  = S01 * L.g[0] + S11 * L.g[1] + S12 * L.g[2];
-        const T SLz  = S02 * L.g[0] + S12 * L.g[1] + S22 * L.g[2];
-        const T advx = U.g[0][0] * ux + U.g[0][1] * uy + U.g[0][2] * uz;
-        const T advy = U.g[1][0] * ux + U.g[1][1] * uy + U.g[1][2] * uz;
-        const T advz = U.g[2][0] * ux + U.g[2][1] * uy + U.g[2][2] * uz;
-        r[1] = -advx - cs2 * px + inv_rho * jxBx +
-               p.nu * (U.lap[0] + (T)2 * SLx) + p.visc_gd * U.gd[0];
-        r[2] = -advy - cs2 * py + inv_rho * jxBy +
-               p.nu * (U.lap[1] + (T)2 * SLy) + p.visc_gd * U.gd[1];
-        r[3] = -advz - cs2 * pz + inv_rho * jxBz +
-               p.nu * (U.lap[2] + (T)2 * SLz) + p.visc_gd * U.gd[2];
-    }
-
-    /* entropy */
-    {
-        const T SS = S00 * S00 + S11 * S11 + S22 * S22 +
-                     (T)2 * (S01 * S01 + S02 * S02 + S12 * S12);
-        const T jj = jx * jx + jy * jy + jz * jz;
-        /* (rho T)^-1 (eta mu0 j.j + 2 rho nu S:S + zeta rho divu^2) */
-        const T heating = inv_T * (inv_rho * p.eta_mu0 * jj + (T)2 * p.nu * SS +
-                                   p.zeta * divu * divu);
-        /* heat conduction: K/rho (first + second.third); the reference's
-         * third term gamma (grad s/cp + grad lnrho) - grad lnrho equals its
-         * second term, so the dot product is a square. */
-        const T first = p.gamma_inv_cp * Sg.lap + p.gamma_m1 * L.lap;
-        T dot2        = 0;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const T second = p.gamma_inv_cp * Sg.g[a] + p.gamma_m1 * L.g[a];
-            dot2 += second * second;
-        }
-        const T heat = p.K * inv_rho * (first + dot2);
-        r[7] = -(ux * Sg.g[0] + uy * Sg.g[1] + uz * Sg.g[2]) + heating + heat;
-    }
+    HydroToMag<T> x;
+    Strain<T> S;
+    MagToHydro<T> m;
+    hydro_prepare(L, Sg.v, U, p, x, S);
+    mag_prepare(Sg, A, p, m);
+    T rh[4], rm[4];
+    hydro_rates(L, U, S, x, m, p, rh);
+    mag_rates(Sg, A, m, x, p, rm);
+    r[0] = rh[0];
+    r[1] = rh[1];
+    r[2] = rh[2];
+    r[3] = rh[3];
+    r[4] = rm[0];
+    r[5] = rm[1];
+    r[6] = rm[2];
+    r[7] = rm[3];
 }

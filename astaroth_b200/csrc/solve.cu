@@ -114,6 +114,11 @@ solve_plain_kernel(const Geom g, const Fields64 f, const StencilCoef sc, const P
     const long long idx = (long long)(i + NGHOST) + (long long)(j + NGHOST) * g.mx +
                           (long long)(k + NGHOST) * g.mxy;
     const long long st[3] = {1, (long long)g.mx, g.mxy};
+    /* previous-substep values, loaded before any store so the loads overlap */
+    double prev[AC_NF];
+#pragma unroll
+    for (int q = 0; q < AC_NF; ++q)
+        prev[q] = rk.step > 0 ? f.out[q][idx] : 0.0;
 
     ScalD<double> L, S;
     VecD<double> U, A;
@@ -137,7 +142,7 @@ solve_plain_kernel(const Geom g, const Fields64 f, const StencilCoef sc, const P
         const double fv = val[q];
         double upd      = rk.dt * r[q];
         if (rk.step > 0)
-            upd = fma(rk.ab, fv - f.out[q][idx], upd);
+            upd = fma(rk.ab, fv - prev[q], upd);
         f.out[q][idx] = fma(rk.beta, upd, fv);
     }
 }

@@ -9,8 +9,13 @@
  * included -- into a slot and signals an mbarrier; every cell value is read
  * from HBM/L2 once per plane per CTA instead of once per stencil tap.
  *
- * The per-cell work (stencils, RHS, single-pass RK3 update) is the one of the
- * plain kernel in solve.cu, reading taps from shared memory.  Reference:
+ * Two warp groups share every cell (256 threads for 128 cells): warps 0-3
+ * evaluate the stencils of lnrho and uu and the continuity and momentum
+ * equations, warps 4-7 those of aa and entropy and the induction and entropy
+ * equations; the two exchange 11 + 9 values per cell through shared memory
+ * between the halves of the RHS.  This doubles the warps per SM (the plane
+ * ring fills the SM's shared memory, so one CTA fits) without extra loads.
+ * The per-cell arithmetic is the one of the plain kernel in solve.cu.  Reference:
  * singlepass_solve / twopass_solve_intermediate,
  * acc-runtime/samples/mhd_modular/mhdsolver.ac:524-612 (the reference issues
  * every tap as a separate __ldg, acc-runtime/acc/stencilgen.c:2205).
@@ -35,7 +40,10 @@ constexpr int SLOT  = AC_NF * PLANE;  /* doubles per ring slot */
 constexpr int RING  = 8;
 constexpr int ZCHUNK = 64;
 constexpr unsigned SLOT_BYTES = SLOT * sizeof(double);
-constexpr size_t SMEM_BYTES   = (size_t)RING * SLOT_BYTES + RING * sizeof(uint64_t);
+constexpr int NCELL = TX * TY;          /* cells per tile, one per thread of a group */
+constexpr int XCHG  = (AC_H2M_COUNT + AC_M2H_COUNT) * NCELL; /* exchange doubles */
+constexpr size_t SMEM_BYTES = (size_t)RING * SLOT_BYTES + (size_t)XCHG * sizeof(double) +
+                              RING * sizeof(uint64_t);
 /* try_wait may suspend the thread for a short, implementation-defined time per
  * call; 2^22 calls bound a wait to seconds even if a copy never lands. */
 constexpr long long kWaitLimit = 1LL << 22;
@@ -196,19 +204,24 @@ vec_derivs(const Taps& t, const int q0, const StencilCoef& sc, VecD<double>& o)
     o.gd[2] = dmix<0, 2>(t, q0, sc.mix[1]) + dmix<1, 2>(t, q0 + 1, sc.mix[2]) + diag[2];
 }
 
-__global__ void __launch_bounds__(TX * TY, 1)
+__global__ void __launch_bounds__(2 * TX * TY, 1)
 solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const Fields64 f,
                    const StencilCoef sc, const PhysConst pc, const RkCoef rk, int* err)
 {
     extern __shared__ __align__(128) double smem[];
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)RING * SLOT);
-    const int lx = threadIdx.x, ly = threadIdx.y;
-    const int tid = ly * TX + lx;
+    double* xh     = smem + (size_t)RING * SLOT;        /* hydro -> magnetic, [value][cell] */
+    double* xm     = xh + (size_t)AC_H2M_COUNT * NCELL; /* magnetic -> hydro */
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)RING * SLOT + XCHG);
+    const int lx = threadIdx.x;
+    const int ly = threadIdx.y & (TY - 1);
+    const int group = threadIdx.y / TY; /* 0: lnrho + uu, 1: aa + entropy (warp uniform) */
+    const int tid   = threadIdx.y * TX + lx;
+    const int cell  = ly * TX + lx;
     const int x0  = blockIdx.x * TX;
     const int y0  = blockIdx.y * TY;
     const int z0  = blockIdx.z * ZCHUNK;
     const int z1  = min(z0 + ZCHUNK, g.nz);
-    const int pfirst = z0 - NGHOST;    /* first plane needed (interior z index) */
+    const int pfirst = z0 - NGHOST;     /* first plane needed (interior z index) */
     const int plast  = z1 - 1 + NGHOST; /* last plane needed */
 
     if (tid == 0) {
@@ -230,10 +243,25 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
     const bool active = x < g.nx && y < g.ny;
     const PhysT<double> p = phys_cast<double>(pc);
     const int cell_off    = (ly + NGHOST) * HX + (lx + NGHOST);
+    /* the 4 output fields of this group, selected with constant indices (a
+     * runtime index into the by-value parameter array would copy it to the stack) */
+    double* outp[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        outp[k] = group == 0 ? f.out[k] : f.out[4 + k];
     bool ok               = true;
     int waited            = pfirst - 1;
 
     for (int z = z0; z < z1; ++z) {
+        const long long idx = (long long)(x + NGHOST) + (long long)(y + NGHOST) * g.mx +
+                              (long long)(z + NGHOST) * g.mxy;
+        /* previous-substep values, loaded early so their latency hides behind the stencils */
+        double prev[4] = {0, 0, 0, 0};
+        if (active && rk.step > 0) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                prev[k] = outp[k][idx];
+        }
         for (int q = waited + 1; q <= z + NGHOST; ++q) {
             const int s = (q - pfirst) & (RING - 1);
             /* after one failed wait the kernel stops waiting and only runs out */
@@ -248,27 +276,62 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
         for (int k = 0; k < 7; ++k)
             t.off[k] = ((z - NGHOST + k - pfirst) & (RING - 1)) * SLOT + cell_off;
 
+        ScalD<double> sd;
+        VecD<double> vd;
+        HydroToMag<double> hx;
+        MagToHydro<double> mx;
+        Strain<double> st;
         if (active) {
-            ScalD<double> L, S;
-            VecD<double> U, A;
-            scal_derivs(t, VTXBUF_LNRHO, sc, L);
-            scal_derivs(t, VTXBUF_ENTROPY, sc, S);
-            vec_derivs(t, VTXBUF_UUX, sc, U);
-            vec_derivs(t, VTXBUF_AX, sc, A);
-            double r[AC_NF];
-            mhd_rates(L, S, U, A, p, r);
-            const double val[AC_NF] = {L.v, U.v[0], U.v[1], U.v[2], A.v[0], A.v[1], A.v[2], S.v};
-            const long long idx = (long long)(x + NGHOST) + (long long)(y + NGHOST) * g.mx +
-                                  (long long)(z + NGHOST) * g.mxy;
+            if (group == 0) {
+                scal_derivs(t, VTXBUF_LNRHO, sc, sd);
+                vec_derivs(t, VTXBUF_UUX, sc, vd);
+                hydro_prepare(sd, t(VTXBUF_ENTROPY, 0, 0, 0), vd, p, hx, st);
 #pragma unroll
-            for (int qf = 0; qf < AC_NF; ++qf) {
-                double upd = rk.dt * r[qf];
-                if (rk.step > 0)
-                    upd = fma(rk.ab, val[qf] - f.out[qf][idx], upd);
-                f.out[qf][idx] = fma(rk.beta, upd, val[qf]);
+                for (int k = 0; k < AC_H2M_COUNT; ++k)
+                    xh[k * NCELL + cell] = hx.a[k];
+            }
+            else {
+                scal_derivs(t, VTXBUF_ENTROPY, sc, sd);
+                vec_derivs(t, VTXBUF_AX, sc, vd);
+                mag_prepare(sd, vd, p, mx);
+#pragma unroll
+                for (int k = 0; k < AC_M2H_COUNT; ++k)
+                    xm[k * NCELL + cell] = mx.a[k];
             }
         }
-        __syncthreads(); /* every thread is done with plane z - 3 */
+        __syncthreads(); /* exchange records written */
+        if (active) {
+            double r[4], val[4];
+            if (group == 0) {
+#pragma unroll
+                for (int k = 0; k < AC_M2H_COUNT; ++k)
+                    mx.a[k] = xm[k * NCELL + cell];
+                hydro_rates(sd, vd, st, hx, mx, p, r);
+                val[0] = sd.v;
+                val[1] = vd.v[0];
+                val[2] = vd.v[1];
+                val[3] = vd.v[2];
+            }
+            else {
+#pragma unroll
+                for (int k = 0; k < AC_H2M_COUNT; ++k)
+                    hx.a[k] = xh[k * NCELL + cell];
+                mag_rates(sd, vd, mx, hx, p, r);
+                val[0] = vd.v[0];
+                val[1] = vd.v[1];
+                val[2] = vd.v[2];
+                val[3] = sd.v;
+            }
+            /* group 0 writes lnrho, ux, uy, uz; group 1 writes ax, ay, az, entropy */
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                double upd = rk.dt * r[k];
+                if (rk.step > 0)
+                    upd = fma(rk.ab, val[k] - prev[k], upd);
+                outp[k][idx] = fma(rk.beta, upd, val[k]);
+            }
+        }
+        __syncthreads(); /* every thread is done with plane z - 3 and the exchange */
         const int next = z - NGHOST + RING;
         if (tid == 0 && next <= plast) {
             const int s = (next - pfirst) & (RING - 1);
@@ -343,7 +406,7 @@ ac_launch_solve64_tiled(const Geom& g, const void* tmap_in, const Fields64& f,
                         const StencilCoef& sc, const PhysConst& pc, const RkCoef& rk, int* err,
                         cudaStream_t stream, unsigned long long* launches)
 {
-    const dim3 tpb(TX, TY, 1);
+    const dim3 tpb(TX, 2 * TY, 1);
     const dim3 bpg((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + ZCHUNK - 1) / ZCHUNK);
     solve_tiled_kernel<<<bpg, tpb, SMEM_BYTES, stream>>>(*(const CUtensorMap*)tmap_in, g, f, sc,
                                                          pc, rk, err);
