@@ -1,5 +1,6 @@
 /*
- * Periodic halo fill and buffer fill kernels.
+ * Periodic halo fill, buffer fills and the FP64 <-> FP32-compensated
+ * conversions of one field.
  *
  * Periodic boundconds: every ghost cell of [start, end) takes the value of
  * the interior cell it wraps to; interior cells are never written, so the
@@ -10,7 +11,7 @@
  * wraps, which differs from the host model on non-cubic grids; this file
  * follows the host model on all grids.
  *
- * One launch fills all requested fields (the reference launches once per
+ * One launch fills all requested arrays (the reference launches once per
  * field, src/core/device.cc:999-1017).  For the whole-mesh box the threads
  * enumerate only the ghost cells (z slabs, then y slabs, then x slabs), so
  * no thread is spent on the interior.
@@ -19,39 +20,45 @@
 
 namespace {
 
-struct FieldList {
-    double* p[AC_NF];
+constexpr int kMaxArrays = 2 * AC_NF; /* FP32 compensated: hi and lo of 8 fields */
+
+template <typename T>
+struct ArrayList {
+    T* p[kMaxArrays];
     int n;
 };
 
+template <typename T>
 __device__ __forceinline__ void
-copy_wrapped(const Geom& g, const FieldList& fl, const int i, const int j, const int k)
+copy_wrapped(const Geom& g, const ArrayList<T>& fl, const int i, const int j, const int k)
 {
     const int is = (i - NGHOST + g.nx) % g.nx + NGHOST;
     const int js = (j - NGHOST + g.ny) % g.ny + NGHOST;
     const int ks = (k - NGHOST + g.nz) % g.nz + NGHOST;
-    const long long dst = (long long)i + (long long)j * g.mx + (long long)k * g.mxy;
-    const long long src = (long long)is + (long long)js * g.mx + (long long)ks * g.mxy;
+    const long long dst = geom_idx(g, i, j, k);
+    const long long src = geom_idx(g, is, js, ks);
 #pragma unroll
-    for (int q = 0; q < AC_NF; ++q)
+    for (int q = 0; q < kMaxArrays; ++q)
         if (q < fl.n)
             fl.p[q][dst] = fl.p[q][src];
 }
 
 /* Whole mesh: t enumerates the ghost cells only. */
+template <typename T>
 __global__ void
-periodic_halo_kernel(const Geom g, const FieldList fl, const long long nzs, const long long nys,
-                     const long long total)
+periodic_halo_kernel(const Geom g, const ArrayList<T> fl, const long long nzs,
+                     const long long nys, const long long total)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= total)
         return;
+    const long long mxy = (long long)g.mx * g.my;
     int i, j, k;
     if (t < nzs) { /* z slabs: 2*NGHOST full planes */
-        i             = (int)(t % g.mx);
-        j             = (int)((t / g.mx) % g.my);
-        const int kk  = (int)(t / g.mxy);
-        k             = kk < NGHOST ? kk : g.nz + kk;
+        i            = (int)(t % g.mx);
+        j            = (int)((t / g.mx) % g.my);
+        const int kk = (int)(t / mxy);
+        k            = kk < NGHOST ? kk : g.nz + kk;
     }
     else if (t < nzs + nys) { /* y slabs inside the interior z range */
         const long long u = t - nzs;
@@ -71,8 +78,9 @@ periodic_halo_kernel(const Geom g, const FieldList fl, const long long nzs, cons
 }
 
 /* General box [start, end): interior cells are skipped. */
+template <typename T>
 __global__ void
-periodic_box_kernel(const Geom g, const FieldList fl, const int3 start, const int3 dims)
+periodic_box_kernel(const Geom g, const ArrayList<T> fl, const int3 start, const int3 dims)
 {
     const int i = start.x + (int)(threadIdx.x + blockIdx.x * blockDim.x);
     const int j = start.y + (int)(threadIdx.y + blockIdx.y * blockDim.y);
@@ -93,45 +101,105 @@ fill_kernel(double* p, const long long count, const double value)
         p[t] = value;
 }
 
+__global__ void
+fill_comp_kernel(float* hi, float* lo, const long long count, const float h, const float l)
+{
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < count;
+         t += (long long)gridDim.x * blockDim.x) {
+        hi[t] = h;
+        lo[t] = l;
+    }
+}
+
+/* One field: double (host layout, pitch mx) -> (hi, lo) with pitch px. */
+__global__ void
+split_kernel(const Geom g, const double* __restrict__ src, float* __restrict__ hi,
+             float* __restrict__ lo)
+{
+    const long long rows = (long long)g.my * g.mz;
+    for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+        const double* s = src + r * g.mx;
+        float* h        = hi + r * g.px;
+        float* l        = lo + r * g.px;
+        for (int i = threadIdx.x; i < g.mx; i += blockDim.x) {
+            const double v = s[i];
+            const float vh = (float)v;
+            h[i]           = vh;
+            l[i]           = (float)(v - (double)vh);
+        }
+    }
+}
+
+__global__ void
+join_kernel(const Geom g, const float* __restrict__ hi, const float* __restrict__ lo,
+            double* __restrict__ dst)
+{
+    const long long rows = (long long)g.my * g.mz;
+    for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
+        double* d       = dst + r * g.mx;
+        const float* h  = hi + r * g.px;
+        const float* l  = lo + r * g.px;
+        for (int i = threadIdx.x; i < g.mx; i += blockDim.x)
+            d[i] = (double)h[i] + (double)l[i];
+    }
+}
+
+int
+grid_for(const long long work, const int tpb)
+{
+    long long bpg = (work + tpb - 1) / tpb;
+    if (bpg > 148LL * 32)
+        bpg = 148LL * 32;
+    return (int)(bpg > 0 ? bpg : 1);
+}
+
 } // namespace
 
+template <typename T>
 cudaError_t
-ac_launch_periodic(const Geom& g, double* const* fields, const int nfields, const Volume start,
+ac_launch_periodic(const Geom& g, T* const* arrays, const int n, const Volume start,
                    const Volume end, cudaStream_t stream, unsigned long long* launches)
 {
-    if (nfields <= 0 || nfields > AC_NF)
+    if (n <= 0 || n > kMaxArrays)
         return cudaErrorInvalidValue;
     if (end.x > (size_t)g.mx || end.y > (size_t)g.my || end.z > (size_t)g.mz ||
         start.x >= end.x || start.y >= end.y || start.z >= end.z)
         return cudaErrorInvalidValue;
-    FieldList fl;
-    fl.n = nfields;
-    for (int q = 0; q < AC_NF; ++q)
-        fl.p[q] = q < nfields ? fields[q] : nullptr;
+    ArrayList<T> fl;
+    fl.n = n;
+    for (int q = 0; q < kMaxArrays; ++q)
+        fl.p[q] = q < n ? arrays[q] : nullptr;
 
     const bool whole = start.x == 0 && start.y == 0 && start.z == 0 && end.x == (size_t)g.mx &&
                        end.y == (size_t)g.my && end.z == (size_t)g.mz;
     if (whole) {
-        const long long nzs   = 2LL * NGHOST * g.mxy;
+        const long long nzs   = 2LL * NGHOST * g.mx * g.my;
         const long long nys   = 2LL * NGHOST * g.mx * g.nz;
         const long long nxs   = 2LL * NGHOST * g.ny * g.nz;
         const long long total = nzs + nys + nxs;
         const int tpb         = 256;
         const long long bpg   = (total + tpb - 1) / tpb;
-        periodic_halo_kernel<<<(unsigned)bpg, tpb, 0, stream>>>(g, fl, nzs, nys, total);
+        periodic_halo_kernel<T><<<(unsigned)bpg, tpb, 0, stream>>>(g, fl, nzs, nys, total);
     }
     else {
-        const int3 s  = make_int3((int)start.x, (int)start.y, (int)start.z);
-        const int3 d  = make_int3((int)(end.x - start.x), (int)(end.y - start.y),
+        const int3 s = make_int3((int)start.x, (int)start.y, (int)start.z);
+        const int3 d = make_int3((int)(end.x - start.x), (int)(end.y - start.y),
                                  (int)(end.z - start.z));
         const dim3 tpb(32, 8, 1);
         const dim3 bpg((d.x + 31) / 32, (d.y + 7) / 8, d.z);
-        periodic_box_kernel<<<bpg, tpb, 0, stream>>>(g, fl, s, d);
+        periodic_box_kernel<T><<<bpg, tpb, 0, stream>>>(g, fl, s, d);
     }
     if (launches)
         ++*launches;
     return cudaGetLastError();
 }
+
+template cudaError_t ac_launch_periodic<double>(const Geom&, double* const*, const int,
+                                                const Volume, const Volume, cudaStream_t,
+                                                unsigned long long*);
+template cudaError_t ac_launch_periodic<float>(const Geom&, float* const*, const int,
+                                               const Volume, const Volume, cudaStream_t,
+                                               unsigned long long*);
 
 cudaError_t
 ac_launch_fill(double* ptr, const long long count, const double value, cudaStream_t stream,
@@ -139,11 +207,41 @@ ac_launch_fill(double* ptr, const long long count, const double value, cudaStrea
 {
     if (count <= 0)
         return cudaSuccess;
-    const int tpb      = 256;
-    long long bpg      = (count + tpb - 1) / tpb;
-    if (bpg > 148 * 32)
-        bpg = 148 * 32;
-    fill_kernel<<<(unsigned)bpg, tpb, 0, stream>>>(ptr, count, value);
+    fill_kernel<<<grid_for(count, 256), 256, 0, stream>>>(ptr, count, value);
+    if (launches)
+        ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t
+ac_launch_fill_comp(float* hi, float* lo, const long long count, const double value,
+                    cudaStream_t stream, unsigned long long* launches)
+{
+    if (count <= 0)
+        return cudaSuccess;
+    const float h = (float)value;
+    const float l = (float)(value - (double)h);
+    fill_comp_kernel<<<grid_for(count, 256), 256, 0, stream>>>(hi, lo, count, h, l);
+    if (launches)
+        ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t
+ac_launch_split(const Geom& g, const double* src, float* hi, float* lo, cudaStream_t stream,
+                unsigned long long* launches)
+{
+    split_kernel<<<grid_for((long long)g.my * g.mz * 256, 256), 256, 0, stream>>>(g, src, hi, lo);
+    if (launches)
+        ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t
+ac_launch_join(const Geom& g, const float* hi, const float* lo, double* dst, cudaStream_t stream,
+               unsigned long long* launches)
+{
+    join_kernel<<<grid_for((long long)g.my * g.mz * 256, 256), 256, 0, stream>>>(g, hi, lo, dst);
     if (launches)
         ++*launches;
     return cudaGetLastError();

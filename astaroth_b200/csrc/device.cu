@@ -24,7 +24,7 @@ static const char* kVersion = "astaroth_b200 0.1 (sm_100a)";
 /* ------------------------------------------------------------------------- */
 
 Geom
-ac_make_geom(const AcMeshInfo& info)
+ac_make_geom(const AcMeshInfo& info, const int precision)
 {
     Geom g;
     const int3 n = info.int3_params[AC_nlocal];
@@ -34,9 +34,73 @@ ac_make_geom(const AcMeshInfo& info)
     g.mx         = n.x + 2 * NGHOST;
     g.my         = n.y + 2 * NGHOST;
     g.mz         = n.z + 2 * NGHOST;
-    g.mxy        = (long long)g.mx * g.my;
-    g.cells      = g.mxy * g.mz;
+    g.px         = precision == 0 ? g.mx : (g.mx + 3) / 4 * 4;
+    g.pxy        = (long long)g.px * g.my;
+    g.cells      = g.pxy * g.mz;
     return g;
+}
+
+/* ---- buffer access ---- */
+
+static size_t
+elem_size(const Device d)
+{
+    return d->precision == 0 ? sizeof(double) : sizeof(float);
+}
+
+static double*
+arr64(const Device d, const int b, const int q)
+{
+    return (double*)d->hi[b] + (size_t)q * d->geom.cells;
+}
+
+static float*
+arr_hi(const Device d, const int b, const int q)
+{
+    return (float*)d->hi[b] + (size_t)q * d->geom.cells;
+}
+
+static float*
+arr_lo(const Device d, const int b, const int q)
+{
+    return d->lo[b] + (size_t)q * d->geom.cells;
+}
+
+static Fields64
+fields64(const Device d)
+{
+    Fields64 f;
+    for (int q = 0; q < AC_NF; ++q) {
+        f.in[q]     = arr64(d, d->in_idx[q], q);
+        f.out[q]    = arr64(d, 1 - d->in_idx[q], q);
+        f.in_lo[q]  = nullptr;
+        f.out_lo[q] = nullptr;
+    }
+    return f;
+}
+
+static Fields32
+fields32(const Device d)
+{
+    Fields32 f;
+    for (int q = 0; q < AC_NF; ++q) {
+        f.in[q]     = arr_hi(d, d->in_idx[q], q);
+        f.out[q]    = arr_hi(d, 1 - d->in_idx[q], q);
+        f.in_lo[q]  = arr_lo(d, d->in_idx[q], q);
+        f.out_lo[q] = arr_lo(d, 1 - d->in_idx[q], q);
+    }
+    return f;
+}
+
+/* The block holding every field's in-buffer (0 or 1), or -1 when single
+ * fields were swapped on their own. */
+static int
+in_block_index(const Device d)
+{
+    for (int q = 1; q < AC_NF; ++q)
+        if (d->in_idx[q] != d->in_idx[0])
+            return -1;
+    return d->in_idx[0];
 }
 
 void
@@ -103,8 +167,11 @@ release(Device d)
     cudaSetDevice(d->id);
     cudaDeviceSynchronize();
     invalidate_graphs(d);
-    cudaFree(d->in_block);
-    cudaFree(d->out_block);
+    for (int b = 0; b < 2; ++b) {
+        cudaFree(d->hi[b]);
+        cudaFree(d->lo[b]);
+    }
+    cudaFree(d->staging);
     cudaFree(d->red.partials);
     cudaFreeHost(d->host_result);
     for (int s = 0; s < NUM_STREAMS; ++s)
@@ -141,8 +208,9 @@ acDeviceCreate(const int id, const AcMeshInfo device_config, Device* device_hand
         return AC_FAILURE;
     }
     const int precision = info.int_params[AC_precision];
-    if (precision != 0) {
-        fprintf(stderr, "astaroth_b200: AC_precision=%d is not supported by this build\n",
+    if (precision != 0 && precision != 1) {
+        fprintf(stderr, "astaroth_b200: AC_precision=%d is not supported (0 FP64, 1 FP32 "
+                        "compensated)\n",
                 precision);
         return AC_FAILURE;
     }
@@ -155,7 +223,7 @@ acDeviceCreate(const int id, const AcMeshInfo device_config, Device* device_hand
     memset(d, 0, dbytes);
     d->id        = id;
     d->config    = info;
-    d->geom      = ac_make_geom(info);
+    d->geom      = ac_make_geom(info, precision);
     d->precision = precision;
     d->solve_variant = info.int_params[AC_debug_plain_kernel] ? 0 : 1;
 
@@ -172,16 +240,21 @@ acDeviceCreate(const int id, const AcMeshInfo device_config, Device* device_hand
     for (int s = 0; s < NUM_STREAMS; ++s)
         CREATE_CHECK(cudaStreamCreateWithFlags(&d->streams[s], cudaStreamNonBlocking));
 
-    const size_t bytes = (size_t)AC_NF * (size_t)d->geom.cells * sizeof(double);
-    CREATE_CHECK(cudaMalloc((void**)&d->in_block, bytes));
-    CREATE_CHECK(cudaMalloc((void**)&d->out_block, bytes));
-    for (int q = 0; q < AC_NF; ++q) {
-        d->f.in[q]  = d->in_block + (size_t)q * d->geom.cells;
-        d->f.out[q] = d->out_block + (size_t)q * d->geom.cells;
+    const size_t bytes = (size_t)AC_NF * (size_t)d->geom.cells * elem_size(d);
+    for (int b = 0; b < 2; ++b) {
+        CREATE_CHECK(cudaMalloc(&d->hi[b], bytes));
+        /* zero-filled in and out, as acVBAReset (acc-runtime/api/vba.cc:274-307) */
+        CREATE_CHECK(cudaMemsetAsync(d->hi[b], 0, bytes, d->streams[0]));
+        if (precision == 1) {
+            CREATE_CHECK(cudaMalloc((void**)&d->lo[b], bytes));
+            CREATE_CHECK(cudaMemsetAsync(d->lo[b], 0, bytes, d->streams[0]));
+        }
     }
-    /* zero-filled in and out, as acVBAReset (acc-runtime/api/vba.cc:274-307) */
-    CREATE_CHECK(cudaMemsetAsync(d->in_block, 0, bytes, d->streams[0]));
-    CREATE_CHECK(cudaMemsetAsync(d->out_block, 0, bytes, d->streams[0]));
+    if (precision == 1)
+        CREATE_CHECK(cudaMalloc((void**)&d->staging, (size_t)d->geom.mx * d->geom.my *
+                                                          d->geom.mz * sizeof(double)));
+    for (int q = 0; q < AC_NF; ++q)
+        d->in_idx[q] = 0;
 
     /* small scratch block: [partials 2*blocks][result 2][counter, err] */
     const int blocks    = ac_reduce_blocks(d->geom);
@@ -192,10 +265,10 @@ acDeviceCreate(const int id, const AcMeshInfo device_config, Device* device_hand
     d->red.result  = d->red.partials + 2 * (size_t)blocks;
     d->red.counter = (unsigned int*)(d->red.result + 2);
     d->err_flag    = (int*)(d->red.counter + 4);
-    d->tmap_ok     = ac_make_tensor_map64(&d->tmap[0], d->in_block, d->geom) &&
-                 ac_make_tensor_map64(&d->tmap[1], d->out_block, d->geom);
+    d->tmap_ok     = ac_make_tensor_map(&d->tmap[0], d->hi[0], d->geom, precision) &&
+                 ac_make_tensor_map(&d->tmap[1], d->hi[1], d->geom, precision);
     if (d->tmap_ok)
-        CREATE_CHECK(ac_solve_tiled_init());
+        CREATE_CHECK(ac_solve_tiled_init(precision));
     CREATE_CHECK(cudaMallocHost((void**)&d->host_result, sizeof(double)));
     CREATE_CHECK(cudaStreamSynchronize(d->streams[0]));
 #undef CREATE_CHECK
@@ -269,9 +342,7 @@ acDeviceSwapBuffer(const Device d, const VertexBufferHandle h)
 {
     if (!d || (int)h < 0 || h >= NUM_VTXBUF_HANDLES)
         return AC_FAILURE;
-    double* t   = d->f.in[h];
-    d->f.in[h]  = d->f.out[h];
-    d->f.out[h] = t;
+    d->in_idx[h] = 1 - d->in_idx[h];
     return AC_SUCCESS;
 }
 
@@ -293,7 +364,7 @@ refresh_config(Device d, const AcMeshInfo& info)
     AcMeshInfo next = info;
     if (acHostUpdateParams(&next) != AC_SUCCESS)
         return AC_FAILURE;
-    const Geom g = ac_make_geom(next);
+    const Geom g = ac_make_geom(next, d->precision);
     if (g.nx != d->geom.nx || g.ny != d->geom.ny || g.nz != d->geom.nz) {
         fprintf(stderr, "astaroth_b200: mesh dimensions cannot change after acDeviceCreate\n");
         return AC_FAILURE;
@@ -401,9 +472,22 @@ acDeviceLoadVertexBuffer(const Device d, const Stream stream, const AcMesh host_
         return AC_FAILURE;
     }
     AC_CUDA_CHECK(cudaSetDevice(d->id));
-    AC_CUDA_CHECK(cudaMemcpyAsync(d->f.in[h], host_mesh.vertex_buffer[h],
-                                  (size_t)d->geom.cells * sizeof(double),
-                                  cudaMemcpyHostToDevice, d->streams[stream]));
+    const size_t n = (size_t)d->geom.mx * d->geom.my * d->geom.mz;
+    const int b    = d->in_idx[h];
+    if (d->precision == 0) {
+        AC_CUDA_CHECK(cudaMemcpyAsync(arr64(d, b, h), host_mesh.vertex_buffer[h],
+                                      n * sizeof(double), cudaMemcpyHostToDevice,
+                                      d->streams[stream]));
+    }
+    else {
+        /* through the staging field: double -> (hi, lo) on the device */
+        AC_CUDA_CHECK(cudaMemcpyAsync(d->staging, host_mesh.vertex_buffer[h], n * sizeof(double),
+                                      cudaMemcpyHostToDevice, d->streams[stream]));
+        AC_CUDA_CHECK(ac_launch_split(d->geom, d->staging, arr_hi(d, b, h), arr_lo(d, b, h),
+                                      d->streams[stream], &d->launches));
+        /* the staging field is shared by all streams: finish before returning */
+        AC_CUDA_CHECK(cudaStreamSynchronize(d->streams[stream]));
+    }
     return AC_SUCCESS;
 }
 
@@ -429,9 +513,19 @@ acDeviceStoreVertexBuffer(const Device d, const Stream stream, const VertexBuffe
         return AC_FAILURE;
     }
     AC_CUDA_CHECK(cudaSetDevice(d->id));
-    AC_CUDA_CHECK(cudaMemcpyAsync(host_mesh->vertex_buffer[h], d->f.in[h],
-                                  (size_t)d->geom.cells * sizeof(double),
-                                  cudaMemcpyDeviceToHost, d->streams[stream]));
+    const size_t n = (size_t)d->geom.mx * d->geom.my * d->geom.mz;
+    const int b    = d->in_idx[h];
+    if (d->precision == 0) {
+        AC_CUDA_CHECK(cudaMemcpyAsync(host_mesh->vertex_buffer[h], arr64(d, b, h),
+                                      n * sizeof(double), cudaMemcpyDeviceToHost,
+                                      d->streams[stream]));
+    }
+    else {
+        AC_CUDA_CHECK(ac_launch_join(d->geom, arr_hi(d, b, h), arr_lo(d, b, h), d->staging,
+                                     d->streams[stream], &d->launches));
+        AC_CUDA_CHECK(cudaMemcpyAsync(host_mesh->vertex_buffer[h], d->staging, n * sizeof(double),
+                                      cudaMemcpyDeviceToHost, d->streams[stream]));
+    }
     /* The host array is ready when the call returns. */
     AC_CUDA_CHECK(cudaStreamSynchronize(d->streams[stream]));
     return AC_SUCCESS;
@@ -453,8 +547,30 @@ acDeviceSetVertexBuffer(const Device d, const Stream stream, const VertexBufferH
     if (!d || !stream_ok(stream) || (int)h < 0 || h >= NUM_VTXBUF_HANDLES)
         return AC_FAILURE;
     AC_CUDA_CHECK(cudaSetDevice(d->id));
-    AC_CUDA_CHECK(ac_launch_fill(d->f.in[h], d->geom.cells, value, d->streams[stream],
-                                 &d->launches));
+    const int b = d->in_idx[h];
+    if (d->precision == 0)
+        AC_CUDA_CHECK(ac_launch_fill(arr64(d, b, h), d->geom.cells, value, d->streams[stream],
+                                     &d->launches));
+    else
+        AC_CUDA_CHECK(ac_launch_fill_comp(arr_hi(d, b, h), arr_lo(d, b, h), d->geom.cells, value,
+                                          d->streams[stream], &d->launches));
+    return AC_SUCCESS;
+}
+
+/* Zero-fills the in and/or out buffer of every field (value and compensation). */
+static AcResult
+clear_buffers(const Device d, cudaStream_t st, const bool in, const bool out)
+{
+    const size_t bytes = (size_t)d->geom.cells * elem_size(d);
+    for (int q = 0; q < AC_NF; ++q)
+        for (int side = 0; side < 2; ++side) {
+            if ((side == 0 && !in) || (side == 1 && !out))
+                continue;
+            const int b = side == 0 ? d->in_idx[q] : 1 - d->in_idx[q];
+            AC_CUDA_CHECK(cudaMemsetAsync((char*)d->hi[b] + q * bytes, 0, bytes, st));
+            if (d->precision == 1)
+                AC_CUDA_CHECK(cudaMemsetAsync(arr_lo(d, b, q), 0, bytes, st));
+        }
     return AC_SUCCESS;
 }
 
@@ -464,10 +580,7 @@ acDeviceFlushOutputBuffers(const Device d, const Stream stream)
     if (!d || !stream_ok(stream))
         return AC_FAILURE;
     AC_CUDA_CHECK(cudaSetDevice(d->id));
-    for (int q = 0; q < AC_NF; ++q)
-        AC_CUDA_CHECK(cudaMemsetAsync(d->f.out[q], 0, (size_t)d->geom.cells * sizeof(double),
-                                      d->streams[stream]));
-    return AC_SUCCESS;
+    return clear_buffers(d, d->streams[stream], false, true);
 }
 
 extern "C" AcResult
@@ -476,13 +589,7 @@ acDeviceResetMesh(const Device d, const Stream stream)
     if (!d || !stream_ok(stream))
         return AC_FAILURE;
     AC_CUDA_CHECK(cudaSetDevice(d->id));
-    for (int q = 0; q < AC_NF; ++q) {
-        AC_CUDA_CHECK(cudaMemsetAsync(d->f.in[q], 0, (size_t)d->geom.cells * sizeof(double),
-                                      d->streams[stream]));
-        AC_CUDA_CHECK(cudaMemsetAsync(d->f.out[q], 0, (size_t)d->geom.cells * sizeof(double),
-                                      d->streams[stream]));
-    }
-    return AC_SUCCESS;
+    return clear_buffers(d, d->streams[stream], true, true);
 }
 
 /* ---- integration ---- */
@@ -509,23 +616,6 @@ rk_coef(const int step, const double dt)
     return rk;
 }
 
-/* Which buffer block holds every field's in-buffer: 0 = in_block, 1 = out_block,
- * -1 = mixed (a single field was swapped on its own). */
-static int
-in_block_index(const Device d)
-{
-    int idx = -1;
-    for (int q = 0; q < AC_NF; ++q) {
-        const int b = d->f.in[q] == d->in_block + (size_t)q * d->geom.cells    ? 0
-                      : d->f.in[q] == d->out_block + (size_t)q * d->geom.cells ? 1
-                                                                                : -1;
-        if (b < 0 || (q > 0 && b != idx))
-            return -1;
-        idx = b;
-    }
-    return idx;
-}
-
 static cudaError_t
 launch_substep(Device d, cudaStream_t st, const int step, const double dt,
                unsigned long long* launches)
@@ -534,11 +624,38 @@ launch_substep(Device d, cudaStream_t st, const int step, const double dt,
     PhysConst pc;
     ac_make_stencil(d->config, &sc);
     ac_make_phys(d->config, &pc);
-    const int blk = in_block_index(d);
-    if (d->solve_variant == 1 && d->tmap_ok && blk >= 0)
-        return ac_launch_solve64_tiled(d->geom, &d->tmap[blk], d->f, sc, pc, rk_coef(step, dt),
-                                       d->err_flag, st, launches);
-    return ac_launch_solve64(d->geom, d->f, sc, pc, rk_coef(step, dt), 0, st, launches);
+    const RkCoef rk = rk_coef(step, dt);
+    const int blk   = in_block_index(d);
+    const bool tiled = d->solve_variant == 1 && d->tmap_ok && blk >= 0;
+    if (d->precision == 0) {
+        const Fields64 f = fields64(d);
+        return tiled ? ac_launch_solve_tiled64(d->geom, &d->tmap[blk], f, sc, pc, rk, d->err_flag,
+                                               st, launches)
+                     : ac_launch_solve_plain64(d->geom, f, sc, pc, rk, st, launches);
+    }
+    const Fields32 f = fields32(d);
+    return tiled ? ac_launch_solve_tiled32(d->geom, &d->tmap[blk], f, sc, pc, rk, d->err_flag, st,
+                                           launches)
+                 : ac_launch_solve_plain32(d->geom, f, sc, pc, rk, st, launches);
+}
+
+/* Periodic halo fill of the in-buffer of fields [q0, q0 + nq). */
+static cudaError_t
+launch_periodic(Device d, cudaStream_t st, const int q0, const int nq, const Volume start,
+                const Volume end, unsigned long long* launches)
+{
+    if (d->precision == 0) {
+        double* a[AC_NF];
+        for (int k = 0; k < nq; ++k)
+            a[k] = arr64(d, d->in_idx[q0 + k], q0 + k);
+        return ac_launch_periodic<double>(d->geom, a, nq, start, end, st, launches);
+    }
+    float* a[2 * AC_NF];
+    for (int k = 0; k < nq; ++k) {
+        a[2 * k]     = arr_hi(d, d->in_idx[q0 + k], q0 + k);
+        a[2 * k + 1] = arr_lo(d, d->in_idx[q0 + k], q0 + k);
+    }
+    return ac_launch_periodic<float>(d->geom, a, 2 * nq, start, end, st, launches);
 }
 
 extern "C" AcResult
@@ -566,9 +683,7 @@ acDevicePeriodicBoundcondStep(const Device d, const Stream stream, const VertexB
     if (!d || !stream_ok(stream) || (int)h < 0 || h >= NUM_VTXBUF_HANDLES)
         return AC_FAILURE;
     AC_CUDA_CHECK(cudaSetDevice(d->id));
-    double* p[1] = {d->f.in[h]};
-    AC_CUDA_CHECK(ac_launch_periodic(d->geom, p, 1, start, end, d->streams[stream],
-                                     &d->launches));
+    AC_CUDA_CHECK(launch_periodic(d, d->streams[stream], h, 1, start, end, &d->launches));
     return AC_SUCCESS;
 }
 
@@ -579,8 +694,7 @@ acDevicePeriodicBoundconds(const Device d, const Stream stream, const Volume sta
     if (!d || !stream_ok(stream))
         return AC_FAILURE;
     AC_CUDA_CHECK(cudaSetDevice(d->id));
-    AC_CUDA_CHECK(ac_launch_periodic(d->geom, d->f.in, AC_NF, start, end, d->streams[stream],
-                                     &d->launches));
+    AC_CUDA_CHECK(launch_periodic(d, d->streams[stream], 0, AC_NF, start, end, &d->launches));
     return AC_SUCCESS;
 }
 
@@ -590,7 +704,7 @@ record_step(Device d, cudaStream_t st, const double dt, unsigned long long* laun
     const Volume m0 = {0, 0, 0};
     const Volume m1 = {(size_t)d->geom.mx, (size_t)d->geom.my, (size_t)d->geom.mz};
     for (int s = 0; s < 3; ++s) {
-        cudaError_t e = ac_launch_periodic(d->geom, d->f.in, AC_NF, m0, m1, st, launches);
+        cudaError_t e = launch_periodic(d, st, 0, AC_NF, m0, m1, launches);
         if (e != cudaSuccess)
             return e;
         e = launch_substep(d, st, s, dt, launches);
@@ -667,12 +781,21 @@ reduce_common(const Device d, const Stream stream, const AcReduction r, const in
     for (int s = 0; s < NUM_STREAMS; ++s)
         if (s != (int)stream)
             AC_CUDA_CHECK(cudaStreamSynchronize(d->streams[s]));
-    const double* fp[4];
-    for (int q = 0; q < kind; ++q)
-        fp[q] = d->f.in[h[q]];
+    const void* fp[4];
+    const float* lo[4] = {nullptr, nullptr, nullptr, nullptr};
+    for (int q = 0; q < kind; ++q) {
+        const int b = d->in_idx[h[q]];
+        if (d->precision == 0) {
+            fp[q] = arr64(d, b, h[q]);
+        }
+        else {
+            fp[q] = arr_hi(d, b, h[q]);
+            lo[q] = arr_lo(d, b, h[q]);
+        }
+    }
     cudaStream_t st = d->streams[stream];
-    AC_CUDA_CHECK(ac_launch_reduce(d->geom, fp, kind, map, r.reduce_op, d->red, st,
-                                   &d->launches));
+    AC_CUDA_CHECK(ac_launch_reduce(d->geom, fp, lo, kind, d->precision, map, r.reduce_op, d->red,
+                                   st, &d->launches));
     AC_CUDA_CHECK(cudaMemcpyAsync(d->host_result, d->red.result, sizeof(double),
                                   cudaMemcpyDeviceToHost, st));
     AC_CUDA_CHECK(cudaStreamSynchronize(st));
@@ -759,8 +882,12 @@ acDeviceGetVertexBufferPtrs(Device d, const VertexBufferHandle h, AcReal** in, A
 {
     if (!d || !in || !out || (int)h < 0 || h >= NUM_VTXBUF_HANDLES)
         return AC_FAILURE;
-    *in  = d->f.in[h];
-    *out = d->f.out[h];
+    if (d->precision != 0) {
+        fprintf(stderr, "astaroth_b200: acDeviceGetVertexBufferPtrs needs an FP64 device\n");
+        return AC_FAILURE;
+    }
+    *in  = arr64(d, d->in_idx[h], h);
+    *out = arr64(d, 1 - d->in_idx[h], h);
     return AC_SUCCESS;
 }
 

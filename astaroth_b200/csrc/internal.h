@@ -25,13 +25,23 @@
         }                                                                                     \
     } while (0)
 
-/* Geometry of one mesh: interior n, allocated m = n + 2*NGHOST, x fastest. */
+/* Geometry of one mesh: interior n, allocated m = n + 2*NGHOST per axis, x
+ * fastest.  Rows are `px` elements apart (px >= mx); FP64 meshes use the host
+ * layout (px = mx), FP32 meshes round px up to a multiple of 4 so every row
+ * starts on a 16-byte boundary (a TMA requirement). */
 struct Geom {
     int nx, ny, nz;
     int mx, my, mz;
-    long long mxy;   /* mx*my */
-    long long cells; /* mx*my*mz */
+    int px;          /* row pitch in elements */
+    long long pxy;   /* px*my: plane pitch in elements */
+    long long cells; /* px*my*mz: elements per field */
 };
+
+__host__ __device__ inline long long
+geom_idx(const Geom& g, const int i, const int j, const int k)
+{
+    return (long long)i + (long long)j * g.px + (long long)k * g.pxy;
+}
 
 /* Physics constants of the RHS, precomputed on the host in double.  The
  * names follow the reference's run_const params
@@ -48,11 +58,29 @@ struct PhysConst {
 };
 
 /* Stencil coefficients with the grid spacing folded in (6th order). */
-struct StencilCoef {
-    double d1[3][3];  /* [axis][k-1] = c_k / ds_axis, c = (3/4, -3/20, 1/60) */
-    double d2[3][4];  /* [axis][k]   = d_k / ds_axis^2, d = (-49/18, 3/2, -3/20, 1/90) */
-    double mix[3][3]; /* [xy,xz,yz][k-1] = e_k / (ds_a ds_b), e = (270,-27,2)/720 */
+template <typename T>
+struct StencilT {
+    T d1[3][3];  /* [axis][k-1] = c_k / ds_axis, c = (3/4, -3/20, 1/60) */
+    T d2[3][4];  /* [axis][k]   = d_k / ds_axis^2, d = (-49/18, 3/2, -3/20, 1/90) */
+    T mix[3][3]; /* [xy,xz,yz][k-1] = e_k / (ds_a ds_b), e = (270,-27,2)/720 */
 };
+typedef StencilT<double> StencilCoef;
+
+template <typename T>
+inline StencilT<T>
+stencil_cast(const StencilCoef& s)
+{
+    StencilT<T> o;
+    for (int a = 0; a < 3; ++a) {
+        for (int k = 0; k < 3; ++k) {
+            o.d1[a][k]  = (T)s.d1[a][k];
+            o.mix[a][k] = (T)s.mix[a][k];
+        }
+        for (int k = 0; k < 4; ++k)
+            o.d2[a][k] = (T)s.d2[a][k];
+    }
+    return o;
+}
 
 /* Coefficients of one substep of the 2N RK3 scheme in single-pass form
  * (acc-runtime/stdlib/integrators.h:11-29):
@@ -65,10 +93,18 @@ struct RkCoef {
     int step;
 };
 
-struct Fields64 {
-    double* in[AC_NF];
-    double* out[AC_NF];
+/* Field arrays of one substep.  FP64: `in`/`out` hold the values (lo unused).
+ * FP32 compensated: the value is hi + lo with |lo| <= ulp(hi)/2; stencils read
+ * hi, the RK3 update is carried out on the (hi, lo) pair. */
+template <typename T>
+struct FieldsT {
+    const T* in[AC_NF];
+    const T* in_lo[AC_NF];
+    T* out[AC_NF];
+    T* out_lo[AC_NF];
 };
+typedef FieldsT<double> Fields64;
+typedef FieldsT<float> Fields32;
 
 /* Scratch of the reductions: per-block partials, a completion counter and
  * the device-side result. */
@@ -82,57 +118,78 @@ struct ReduceScratch {
 struct StepGraph {
     cudaGraphExec_t exec;
     double dt;
-    const void* in0; /* in-buffer pointer of field 0 the graph was captured with */
     int valid;
 };
 
+/* The two buffers of every field: block b holds all 8 fields of buffer b
+ * (field q at offset q*cells).  in_idx[q] says which block is field q's
+ * in-buffer; swaps flip it. */
 struct device_s {
-    CUtensorMap tmap[2]; /* 4-D (x, y, z, field) maps of in_block / out_block */
+    CUtensorMap tmap[2]; /* 4-D (x, y, z, field) maps of the value (hi) array of each block */
     int tmap_ok;
     int* err_flag;       /* device word set by kernels whose bounded waits gave up */
     int id;
     AcMeshInfo config;
     Geom geom;
-    int precision;
+    int precision;       /* 0 FP64, 1 FP32 compensated */
     cudaStream_t streams[NUM_STREAMS];
-    double* in_block;
-    double* out_block;
-    Fields64 f;
+    void* hi[2];         /* double* (FP64) or float* (FP32) value arrays per block */
+    float* lo[2];        /* FP32 compensation arrays per block (NULL for FP64) */
+    double* staging;     /* FP32: one field of doubles for host transfers */
+    int in_idx[AC_NF];
     ReduceScratch red;
     double* host_result; /* pinned */
     StepGraph graphs[NUM_STREAMS][2];
-    int solve_variant; /* 0 = plain, 1 = tiled */
+    int solve_variant;   /* 0 = plain, 1 = tiled */
     unsigned long long launches;
 };
 
 /* ---- launchers (each returns the launch error, cudaSuccess on success) ---- */
 
-cudaError_t ac_launch_periodic(const Geom& g, double* const* fields, const int nfields,
-                               const Volume start, const Volume end, cudaStream_t stream,
+/* Periodic halo fill of n arrays of element type T (double or float). */
+template <typename T>
+cudaError_t ac_launch_periodic(const Geom& g, T* const* arrays, const int n, const Volume start,
+                               const Volume end, cudaStream_t stream,
                                unsigned long long* launches);
 
 cudaError_t ac_launch_fill(double* ptr, const long long count, const double value,
                            cudaStream_t stream, unsigned long long* launches);
+/* FP32 compensated: hi/lo of `count` elements from a double value */
+cudaError_t ac_launch_fill_comp(float* hi, float* lo, const long long count, const double value,
+                                cudaStream_t stream, unsigned long long* launches);
+/* FP32 compensated <-> double (host layout, row pitch mx) conversions of one field */
+cudaError_t ac_launch_split(const Geom& g, const double* src, float* hi, float* lo,
+                            cudaStream_t stream, unsigned long long* launches);
+cudaError_t ac_launch_join(const Geom& g, const float* hi, const float* lo, double* dst,
+                           cudaStream_t stream, unsigned long long* launches);
 
-cudaError_t ac_launch_solve64(const Geom& g, const Fields64& f, const StencilCoef& sc,
-                              const PhysConst& pc, const RkCoef& rk, const int variant,
-                              cudaStream_t stream, unsigned long long* launches);
+cudaError_t ac_launch_solve_plain64(const Geom& g, const Fields64& f, const StencilCoef& sc,
+                                    const PhysConst& pc, const RkCoef& rk, cudaStream_t stream,
+                                    unsigned long long* launches);
+cudaError_t ac_launch_solve_plain32(const Geom& g, const Fields32& f, const StencilCoef& sc,
+                                    const PhysConst& pc, const RkCoef& rk, cudaStream_t stream,
+                                    unsigned long long* launches);
 
-/* map: AcKernel of the reduction's map; op: AcReduceOp; fields: up to 4. */
-cudaError_t ac_launch_reduce(const Geom& g, const double* const* fields, const int nfields,
-                             const int map, const int op, const ReduceScratch& scratch,
-                             cudaStream_t stream, unsigned long long* launches);
+/* map: AcKernel of the reduction's map; op: AcReduceOp; up to 4 fields; lo
+ * arrays are NULL for FP64 meshes. */
+cudaError_t ac_launch_reduce(const Geom& g, const void* const* fields, const float* const* lo,
+                             const int nfields, const int precision, const int map,
+                             const int op, const ReduceScratch& scratch, cudaStream_t stream,
+                             unsigned long long* launches);
 
 int ac_reduce_blocks(const Geom& g);
 
-bool ac_tiled_supported(const Geom& g);
-cudaError_t ac_solve_tiled_init();
-bool ac_make_tensor_map64(void* map_out, double* base, const Geom& g);
-cudaError_t ac_launch_solve64_tiled(const Geom& g, const void* tmap_in, const Fields64& f,
+bool ac_tiled_supported(const Geom& g, const int precision);
+bool ac_make_tensor_map(void* map_out, void* base, const Geom& g, const int precision);
+cudaError_t ac_solve_tiled_init(const int precision);
+cudaError_t ac_launch_solve_tiled64(const Geom& g, const void* tmap_in, const Fields64& f,
+                                    const StencilCoef& sc, const PhysConst& pc, const RkCoef& rk,
+                                    int* err, cudaStream_t stream, unsigned long long* launches);
+cudaError_t ac_launch_solve_tiled32(const Geom& g, const void* tmap_in, const Fields32& f,
                                     const StencilCoef& sc, const PhysConst& pc, const RkCoef& rk,
                                     int* err, cudaStream_t stream, unsigned long long* launches);
 
 /* Host-side setup helpers (device.cu). */
 void ac_make_stencil(const AcMeshInfo& info, StencilCoef* sc);
 void ac_make_phys(const AcMeshInfo& info, PhysConst* pc);
-Geom ac_make_geom(const AcMeshInfo& info);
+Geom ac_make_geom(const AcMeshInfo& info, const int precision);

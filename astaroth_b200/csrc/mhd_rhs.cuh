@@ -245,3 +245,44 @@ mhd_rates(const ScalD<T>& L, const ScalD<T>& Sg, const VecD<T>& U, const VecD<T>
     r[6] = rm[2];
     r[7] = rm[3];
 }
+
+/* Single-pass 2N RK3 update of one value (acc-runtime/stdlib/integrators.h:16-29):
+ *   f_new = f + beta (ab (f - f_prev) + dt rate)
+ * FP64: plain arithmetic.  FP32 compensated: f = (h, l) with |l| <= ulp(h)/2;
+ * the increment is formed in FP32 (it is small against f) and added with an
+ * error-free two-sum, so the accumulated state keeps ~48 significant bits. */
+struct RkT64 {
+    double dt, beta, ab;
+};
+struct RkT32 {
+    float dt, beta, ab;
+};
+
+__device__ __forceinline__ void
+rk_update(const double f, const double f_prev, const double rate, const RkT64& c,
+          const bool use_prev, double& out)
+{
+    double upd = c.dt * rate;
+    if (use_prev)
+        upd = fma(c.ab, f - f_prev, upd);
+    out = fma(c.beta, upd, f);
+}
+
+__device__ __forceinline__ void
+rk_update_comp(const float h, const float l, const float ph, const float pl, const float rate,
+               const RkT32& c, const bool use_prev, float& oh, float& ol)
+{
+    float upd = c.dt * rate;
+    if (use_prev) {
+        const float d = (h - ph) + (l - pl);
+        upd           = fmaf(c.ab, d, upd);
+    }
+    const float inc = c.beta * upd;
+    /* two-sum (h, inc) -> (s, e), then fold in l and renormalise */
+    const float s  = __fadd_rn(h, inc);
+    const float bb = __fsub_rn(s, h);
+    const float e  = __fadd_rn(__fsub_rn(h, __fsub_rn(s, bb)), __fsub_rn(inc, bb));
+    const float l2 = __fadd_rn(l, e);
+    oh             = __fadd_rn(s, l2);
+    ol             = __fsub_rn(l2, __fsub_rn(oh, s));
+}

@@ -44,14 +44,29 @@ dd_add(const DD x, const DD y)
     return DD{hi, e - (hi - s)};
 }
 
-struct ReduceFields {
+/* Reads the value of field q at idx: FP64 arrays, or hi + lo of the FP32
+ * compensated representation (exact in double). */
+struct Reader64 {
     const double* p[4];
+    __device__ __forceinline__ double operator()(const int q, const long long idx) const
+    {
+        return p[q][idx];
+    }
+};
+struct ReaderComp {
+    const float* hi[4];
+    const float* lo[4];
+    __device__ __forceinline__ double operator()(const int q, const long long idx) const
+    {
+        return (double)hi[q][idx] + (double)lo[q][idx];
+    }
 };
 
+template <typename R>
 __device__ __forceinline__ double
-map_value(const int map, const ReduceFields& f, const long long idx)
+map_value(const int map, const R& f, const long long idx)
 {
-    const double a = f.p[0][idx];
+    const double a = f(0, idx);
     switch (map) {
     case AC_MAP_VTXBUF:
         return a;
@@ -64,8 +79,8 @@ map_value(const int map, const ReduceFields& f, const long long idx)
     default:
         break;
     }
-    const double b  = f.p[1][idx];
-    const double c  = f.p[2][idx];
+    const double b  = f(1, idx);
+    const double c  = f(2, idx);
     const double sq = a * a + b * b + c * c;
     switch (map) {
     case AC_MAP_VTXBUF3_NORM:
@@ -77,9 +92,9 @@ map_value(const int map, const ReduceFields& f, const long long idx)
         return ea * ea + eb * eb + ec * ec;
     }
     case AC_MAP_VTXBUF4_ALFVEN_NORM:
-        return sqrt(sq) / sqrt(exp(f.p[3][idx]));
+        return sqrt(sq) / sqrt(exp(f(3, idx)));
     case AC_MAP_VTXBUF4_ALFVEN_SQUARE:
-        return sq / exp(f.p[3][idx]);
+        return sq / exp(f(3, idx));
     default:
         return 0;
     }
@@ -91,8 +106,9 @@ combine(const int op, const double a, const double b)
     return op == AC_REDUCE_OP_MAX ? fmax(a, b) : fmin(a, b);
 }
 
+template <typename R>
 __global__ void __launch_bounds__(kTpb)
-reduce_kernel(const Geom g, const ReduceFields f, const int map, const int op,
+reduce_kernel(const Geom g, const R f, const int map, const int op,
               double* __restrict__ partials, unsigned int* __restrict__ counter,
               double* __restrict__ result)
 {
@@ -108,8 +124,7 @@ reduce_kernel(const Geom g, const ReduceFields f, const int map, const int op,
     for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
         const int j          = (int)(r % g.ny);
         const int k          = (int)(r / g.ny);
-        const long long base = NGHOST + (long long)(j + NGHOST) * g.mx +
-                               (long long)(k + NGHOST) * g.mxy;
+        const long long base = geom_idx(g, NGHOST, j + NGHOST, k + NGHOST);
         for (int i = threadIdx.x; i < g.nx; i += kTpb) {
             const double v = map_value(map, f, base + i);
             if (is_sum)
@@ -206,22 +221,33 @@ ac_reduce_blocks(const Geom& g)
 }
 
 cudaError_t
-ac_launch_reduce(const Geom& g, const double* const* fields, const int nfields, const int map,
-                 const int op, const ReduceScratch& scratch, cudaStream_t stream,
-                 unsigned long long* launches)
+ac_launch_reduce(const Geom& g, const void* const* fields, const float* const* lo,
+                 const int nfields, const int precision, const int map, const int op,
+                 const ReduceScratch& scratch, cudaStream_t stream, unsigned long long* launches)
 {
     if (nfields < 1 || nfields > 4)
         return cudaErrorInvalidValue;
     if (op != AC_REDUCE_OP_SUM && op != AC_REDUCE_OP_MAX && op != AC_REDUCE_OP_MIN)
         return cudaErrorInvalidValue;
-    ReduceFields f;
-    for (int q = 0; q < 4; ++q)
-        f.p[q] = fields[q < nfields ? q : 0];
     const int blocks = ac_reduce_blocks(g);
     if (blocks > scratch.max_blocks)
         return cudaErrorInvalidValue;
-    reduce_kernel<<<blocks, kTpb, 0, stream>>>(g, f, map, op, scratch.partials, scratch.counter,
-                                              scratch.result);
+    if (precision == 0) {
+        Reader64 f;
+        for (int q = 0; q < 4; ++q)
+            f.p[q] = (const double*)fields[q < nfields ? q : 0];
+        reduce_kernel<<<blocks, kTpb, 0, stream>>>(g, f, map, op, scratch.partials,
+                                                   scratch.counter, scratch.result);
+    }
+    else {
+        ReaderComp f;
+        for (int q = 0; q < 4; ++q) {
+            f.hi[q] = (const float*)fields[q < nfields ? q : 0];
+            f.lo[q] = lo[q < nfields ? q : 0];
+        }
+        reduce_kernel<<<blocks, kTpb, 0, stream>>>(g, f, map, op, scratch.partials,
+                                                   scratch.counter, scratch.result);
+    }
     if (launches)
         ++*launches;
     return cudaGetLastError();

@@ -1,11 +1,14 @@
 /*
- * FP64 substep kernel, 2.5-D blocked (the production path on B200).
+ * The substep kernel, 2.5-D blocked (the production path on B200), for FP64
+ * meshes and FP32-compensated meshes (the FP32 ring holds the hi parts; the
+ * update works on (hi, lo) pairs, see rk_update_comp).
  *
  * Each CTA owns a 32 x 4 (x, y) tile of the interior and marches along z over
  * a chunk of ZCHUNK planes.  A ring of RING = 8 shared-memory slots holds the
  * planes z-3 .. z+3 the stencils of plane z need plus one plane in flight.
  * One TMA instruction (cp.async.bulk.tensor.4d, no multicast) brings a whole
- * plane of all 8 fields -- a (38 x 10 x 1 x 8) box of the in-buffer, halo
+ * plane of all 8 fields -- a (38 x 10 x 1 x 8) box of the in-buffer (40 wide
+ * in FP32, where the box row must be a multiple of 16 bytes), halo
  * included -- into a slot and signals an mbarrier; every cell value is read
  * from HBM/L2 once per plane per CTA instead of once per stencil tap.
  *
@@ -31,22 +34,41 @@
 
 namespace {
 
-constexpr int TX    = 32;
-constexpr int TY    = 4;
-constexpr int HX    = TX + 2 * NGHOST;
-constexpr int HY    = TY + 2 * NGHOST;
-constexpr int PLANE = HX * HY;        /* doubles per field per plane */
-constexpr int SLOT  = AC_NF * PLANE;  /* doubles per ring slot */
-constexpr int RING  = 8;
+constexpr int TX     = 32;
+constexpr int TY     = 4;
+constexpr int HY     = TY + 2 * NGHOST;
+constexpr int RING   = 8;
 constexpr int ZCHUNK = 64;
-constexpr unsigned SLOT_BYTES = SLOT * sizeof(double);
-constexpr int NCELL = TX * TY;          /* cells per tile, one per thread of a group */
-constexpr int XCHG  = (AC_H2M_COUNT + AC_M2H_COUNT) * NCELL; /* exchange doubles */
-constexpr size_t SMEM_BYTES = (size_t)RING * SLOT_BYTES + (size_t)XCHG * sizeof(double) +
-                              RING * sizeof(uint64_t);
+constexpr int NCELL  = TX * TY; /* cells per tile, one per thread of a group */
+constexpr int XCHG   = (AC_H2M_COUNT + AC_M2H_COUNT) * NCELL; /* exchange entries */
 /* try_wait may suspend the thread for a short, implementation-defined time per
  * call; 2^22 calls bound a wait to seconds even if a copy never lands. */
 constexpr long long kWaitLimit = 1LL << 22;
+
+template <typename T>
+struct Tile;
+template <>
+struct Tile<double> {
+    static constexpr int HXP  = TX + 2 * NGHOST; /* 38 x 8 B = 304 B rows */
+    static constexpr int MINB = 1;
+    static constexpr CUtensorMapDataType kType = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
+};
+template <>
+struct Tile<float> {
+    static constexpr int HXP  = 40; /* 38 rounded up: 160 B rows */
+    static constexpr int MINB = 2;
+    static constexpr CUtensorMapDataType kType = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+};
+
+template <typename T>
+struct Layout {
+    static constexpr int HXP        = Tile<T>::HXP;
+    static constexpr int PLANE      = HXP * HY;    /* elements per field per plane */
+    static constexpr int SLOT       = AC_NF * PLANE; /* elements per ring slot */
+    static constexpr unsigned SLOT_BYTES = SLOT * sizeof(T);
+    static constexpr size_t SMEM_BYTES   = (size_t)RING * SLOT_BYTES + (size_t)XCHG * sizeof(T) +
+                                         RING * sizeof(uint64_t);
+};
 
 __device__ __forceinline__ uint32_t
 smem_addr(const void* p)
@@ -98,7 +120,7 @@ mbar_wait_bounded(uint64_t* bar, const unsigned parity)
 }
 
 __device__ __forceinline__ void
-tma_load_plane(double* dst, const CUtensorMap* map, uint64_t* bar, const int x, const int y,
+tma_load_plane(void* dst, const CUtensorMap* map, uint64_t* bar, const int x, const int y,
                const int z)
 {
     asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
@@ -108,47 +130,48 @@ tma_load_plane(double* dst, const CUtensorMap* map, uint64_t* bar, const int x, 
 }
 
 /* Taps of field q at offset (dx, dy, dz) from this thread's cell. */
+template <typename T>
 struct Taps {
-    const double* s;
+    const T* s;
     int off[7]; /* per dz = -3..3: slot base + this thread's (x, y) position */
-    __device__ __forceinline__ double operator()(const int q, const int dx, const int dy,
-                                                 const int dz) const
+    __device__ __forceinline__ T operator()(const int q, const int dx, const int dy,
+                                            const int dz) const
     {
-        return s[off[dz + 3] + q * PLANE + dy * HX + dx];
+        return s[off[dz + 3] + q * Layout<T>::PLANE + dy * Layout<T>::HXP + dx];
     }
 };
 
-template <int A>
-__device__ __forceinline__ double
-tap1(const Taps& t, const int q, const int k)
+template <int A, typename T>
+__device__ __forceinline__ T
+tap1(const Taps<T>& t, const int q, const int k)
 {
     return A == 0 ? t(q, k, 0, 0) : A == 1 ? t(q, 0, k, 0) : t(q, 0, 0, k);
 }
 
-template <int A>
-__device__ __forceinline__ double
-d1(const Taps& t, const int q, const double* c)
+template <int A, typename T>
+__device__ __forceinline__ T
+d1(const Taps<T>& t, const int q, const T* c)
 {
-    double r = c[0] * (tap1<A>(t, q, 1) - tap1<A>(t, q, -1));
-    r        = fma(c[1], tap1<A>(t, q, 2) - tap1<A>(t, q, -2), r);
-    r        = fma(c[2], tap1<A>(t, q, 3) - tap1<A>(t, q, -3), r);
+    T r = c[0] * (tap1<A>(t, q, 1) - tap1<A>(t, q, -1));
+    r   = fma(c[1], tap1<A>(t, q, 2) - tap1<A>(t, q, -2), r);
+    r   = fma(c[2], tap1<A>(t, q, 3) - tap1<A>(t, q, -3), r);
     return r;
 }
 
-template <int A>
-__device__ __forceinline__ double
-d2_sides(const Taps& t, const int q, const double* d)
+template <int A, typename T>
+__device__ __forceinline__ T
+d2_sides(const Taps<T>& t, const int q, const T* d)
 {
-    double r = d[1] * (tap1<A>(t, q, 1) + tap1<A>(t, q, -1));
-    r        = fma(d[2], tap1<A>(t, q, 2) + tap1<A>(t, q, -2), r);
-    r        = fma(d[3], tap1<A>(t, q, 3) + tap1<A>(t, q, -3), r);
+    T r = d[1] * (tap1<A>(t, q, 1) + tap1<A>(t, q, -1));
+    r   = fma(d[2], tap1<A>(t, q, 2) + tap1<A>(t, q, -2), r);
+    r   = fma(d[3], tap1<A>(t, q, 3) + tap1<A>(t, q, -3), r);
     return r;
 }
 
 /* tap at +a along axis A and +b along axis B (A < B) */
-template <int A, int B>
-__device__ __forceinline__ double
-tap2(const Taps& t, const int q, const int a, const int b)
+template <int A, int B, typename T>
+__device__ __forceinline__ T
+tap2(const Taps<T>& t, const int q, const int a, const int b)
 {
     if (A == 0 && B == 1)
         return t(q, a, b, 0);
@@ -157,22 +180,23 @@ tap2(const Taps& t, const int q, const int a, const int b)
     return t(q, 0, a, b);
 }
 
-template <int A, int B>
-__device__ __forceinline__ double
-dmix(const Taps& t, const int q, const double* e)
+template <int A, int B, typename T>
+__device__ __forceinline__ T
+dmix(const Taps<T>& t, const int q, const T* e)
 {
-    double r = 0;
+    T r = 0;
 #pragma unroll
     for (int k = 1; k <= 3; ++k) {
-        const double s = (tap2<A, B>(t, q, k, k) + tap2<A, B>(t, q, -k, -k)) -
-                         (tap2<A, B>(t, q, k, -k) + tap2<A, B>(t, q, -k, k));
+        const T s = (tap2<A, B>(t, q, k, k) + tap2<A, B>(t, q, -k, -k)) -
+                    (tap2<A, B>(t, q, k, -k) + tap2<A, B>(t, q, -k, k));
         r = k == 1 ? e[0] * s : fma(e[k - 1], s, r);
     }
     return r;
 }
 
+template <typename T>
 __device__ __forceinline__ void
-scal_derivs(const Taps& t, const int q, const StencilCoef& sc, ScalD<double>& o)
+scal_derivs(const Taps<T>& t, const int q, const StencilT<T>& sc, ScalD<T>& o)
 {
     o.v    = t(q, 0, 0, 0);
     o.g[0] = d1<0>(t, q, sc.d1[0]);
@@ -182,10 +206,11 @@ scal_derivs(const Taps& t, const int q, const StencilCoef& sc, ScalD<double>& o)
             d2_sides<1>(t, q, sc.d2[1]) + d2_sides<2>(t, q, sc.d2[2]);
 }
 
+template <typename T>
 __device__ __forceinline__ void
-vec_derivs(const Taps& t, const int q0, const StencilCoef& sc, VecD<double>& o)
+vec_derivs(const Taps<T>& t, const int q0, const StencilT<T>& sc, VecD<T>& o)
 {
-    double diag[3];
+    T diag[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
         const int q = q0 + c;
@@ -193,34 +218,38 @@ vec_derivs(const Taps& t, const int q0, const StencilCoef& sc, VecD<double>& o)
         o.g[c][0]   = d1<0>(t, q, sc.d1[0]);
         o.g[c][1]   = d1<1>(t, q, sc.d1[1]);
         o.g[c][2]   = d1<2>(t, q, sc.d1[2]);
-        const double s0 = d2_sides<0>(t, q, sc.d2[0]);
-        const double s1 = d2_sides<1>(t, q, sc.d2[1]);
-        const double s2 = d2_sides<2>(t, q, sc.d2[2]);
-        diag[c]  = sc.d2[c][0] * o.v[c] + (c == 0 ? s0 : c == 1 ? s1 : s2);
-        o.lap[c] = (sc.d2[0][0] + sc.d2[1][0] + sc.d2[2][0]) * o.v[c] + s0 + s1 + s2;
+        const T s0  = d2_sides<0>(t, q, sc.d2[0]);
+        const T s1  = d2_sides<1>(t, q, sc.d2[1]);
+        const T s2  = d2_sides<2>(t, q, sc.d2[2]);
+        diag[c]     = sc.d2[c][0] * o.v[c] + (c == 0 ? s0 : c == 1 ? s1 : s2);
+        o.lap[c]    = (sc.d2[0][0] + sc.d2[1][0] + sc.d2[2][0]) * o.v[c] + s0 + s1 + s2;
     }
     o.gd[0] = diag[0] + dmix<0, 1>(t, q0 + 1, sc.mix[0]) + dmix<0, 2>(t, q0 + 2, sc.mix[1]);
     o.gd[1] = dmix<0, 1>(t, q0, sc.mix[0]) + diag[1] + dmix<1, 2>(t, q0 + 2, sc.mix[2]);
     o.gd[2] = dmix<0, 2>(t, q0, sc.mix[1]) + dmix<1, 2>(t, q0 + 1, sc.mix[2]) + diag[2];
 }
 
-__global__ void __launch_bounds__(2 * TX * TY, 1)
-solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const Fields64 f,
-                   const StencilCoef sc, const PhysConst pc, const RkCoef rk, int* err)
+template <typename T, bool COMP>
+__global__ void __launch_bounds__(2 * TX * TY, Tile<T>::MINB)
+solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const FieldsT<T> f,
+                   const StencilT<T> sc, const PhysConst pc, const RkCoef rk, int* err)
 {
-    extern __shared__ __align__(128) double smem[];
-    double* xh     = smem + (size_t)RING * SLOT;        /* hydro -> magnetic, [value][cell] */
-    double* xm     = xh + (size_t)AC_H2M_COUNT * NCELL; /* magnetic -> hydro */
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + (size_t)RING * SLOT + XCHG);
-    const int lx = threadIdx.x;
-    const int ly = threadIdx.y & (TY - 1);
+    typedef Layout<T> L;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    T* smem        = reinterpret_cast<T*>(smem_raw);
+    T* xh          = smem + (size_t)RING * L::SLOT;      /* hydro -> magnetic, [value][cell] */
+    T* xm          = xh + (size_t)AC_H2M_COUNT * NCELL;  /* magnetic -> hydro */
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem_raw + (size_t)RING * L::SLOT_BYTES +
+                                                 (size_t)XCHG * sizeof(T));
+    const int lx    = threadIdx.x;
+    const int ly    = threadIdx.y & (TY - 1);
     const int group = threadIdx.y / TY; /* 0: lnrho + uu, 1: aa + entropy (warp uniform) */
     const int tid   = threadIdx.y * TX + lx;
     const int cell  = ly * TX + lx;
-    const int x0  = blockIdx.x * TX;
-    const int y0  = blockIdx.y * TY;
-    const int z0  = blockIdx.z * ZCHUNK;
-    const int z1  = min(z0 + ZCHUNK, g.nz);
+    const int x0    = blockIdx.x * TX;
+    const int y0    = blockIdx.y * TY;
+    const int z0    = blockIdx.z * ZCHUNK;
+    const int z1    = min(z0 + ZCHUNK, g.nz);
     const int pfirst = z0 - NGHOST;     /* first plane needed (interior z index) */
     const int plast  = z1 - 1 + NGHOST; /* last plane needed */
 
@@ -234,33 +263,46 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
         const int pend = min(plast, pfirst + RING - 1);
         for (int p = pfirst; p <= pend; ++p) {
             const int s = (p - pfirst) & (RING - 1);
-            mbar_arrive_expect_tx(&bars[s], SLOT_BYTES);
-            tma_load_plane(smem + (size_t)s * SLOT, &tmap, &bars[s], x0, y0, p + NGHOST);
+            mbar_arrive_expect_tx(&bars[s], L::SLOT_BYTES);
+            tma_load_plane(smem + (size_t)s * L::SLOT, &tmap, &bars[s], x0, y0, p + NGHOST);
         }
     }
 
     const int x = x0 + lx, y = y0 + ly;
-    const bool active = x < g.nx && y < g.ny;
-    const PhysT<double> p = phys_cast<double>(pc);
-    const int cell_off    = (ly + NGHOST) * HX + (lx + NGHOST);
-    /* the 4 output fields of this group, selected with constant indices (a
-     * runtime index into the by-value parameter array would copy it to the stack) */
-    double* outp[4];
+    const bool active  = x < g.nx && y < g.ny;
+    const bool use_prev = rk.step > 0;
+    const PhysT<T> p   = phys_cast<T>(pc);
+    const int cell_off = (ly + NGHOST) * L::HXP + (lx + NGHOST);
+    /* the 4 fields of this group, selected with constant indices (a runtime
+     * index into the by-value parameter arrays would copy them to the stack) */
+    T* outp[4];
+    T* outl[4];
+    const T* inl[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k)
+    for (int k = 0; k < 4; ++k) {
         outp[k] = group == 0 ? f.out[k] : f.out[4 + k];
-    bool ok               = true;
-    int waited            = pfirst - 1;
+        outl[k] = group == 0 ? f.out_lo[k] : f.out_lo[4 + k];
+        inl[k]  = group == 0 ? f.in_lo[k] : f.in_lo[4 + k];
+    }
+    bool ok    = true;
+    int waited = pfirst - 1;
 
     for (int z = z0; z < z1; ++z) {
-        const long long idx = (long long)(x + NGHOST) + (long long)(y + NGHOST) * g.mx +
-                              (long long)(z + NGHOST) * g.mxy;
-        /* previous-substep values, loaded early so their latency hides behind the stencils */
-        double prev[4] = {0, 0, 0, 0};
-        if (active && rk.step > 0) {
+        const long long idx = geom_idx(g, x + NGHOST, y + NGHOST, z + NGHOST);
+        /* previous-substep values (and compensation terms), loaded early so
+         * their latency hides behind the stencils */
+        T prev[4] = {0, 0, 0, 0}, prevl[4] = {0, 0, 0, 0}, lo[4] = {0, 0, 0, 0};
+        if (active) {
 #pragma unroll
-            for (int k = 0; k < 4; ++k)
-                prev[k] = outp[k][idx];
+            for (int k = 0; k < 4; ++k) {
+                if (use_prev)
+                    prev[k] = outp[k][idx];
+                if (COMP) {
+                    lo[k] = inl[k][idx];
+                    if (use_prev)
+                        prevl[k] = outl[k][idx];
+                }
+            }
         }
         for (int q = waited + 1; q <= z + NGHOST; ++q) {
             const int s = (q - pfirst) & (RING - 1);
@@ -270,17 +312,17 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
         }
         waited = z + NGHOST;
 
-        Taps t;
+        Taps<T> t;
         t.s = smem;
 #pragma unroll
         for (int k = 0; k < 7; ++k)
-            t.off[k] = ((z - NGHOST + k - pfirst) & (RING - 1)) * SLOT + cell_off;
+            t.off[k] = ((z - NGHOST + k - pfirst) & (RING - 1)) * L::SLOT + cell_off;
 
-        ScalD<double> sd;
-        VecD<double> vd;
-        HydroToMag<double> hx;
-        MagToHydro<double> mx;
-        Strain<double> st;
+        ScalD<T> sd;
+        VecD<T> vd;
+        HydroToMag<T> hx;
+        MagToHydro<T> mx;
+        Strain<T> st;
         if (active) {
             if (group == 0) {
                 scal_derivs(t, VTXBUF_LNRHO, sc, sd);
@@ -301,7 +343,7 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
         }
         __syncthreads(); /* exchange records written */
         if (active) {
-            double r[4], val[4];
+            T r[4], val[4];
             if (group == 0) {
 #pragma unroll
                 for (int k = 0; k < AC_M2H_COUNT; ++k)
@@ -325,18 +367,27 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
             /* group 0 writes lnrho, ux, uy, uz; group 1 writes ax, ay, az, entropy */
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                double upd = rk.dt * r[k];
-                if (rk.step > 0)
-                    upd = fma(rk.ab, val[k] - prev[k], upd);
-                outp[k][idx] = fma(rk.beta, upd, val[k]);
+                if constexpr (COMP) {
+                    const RkT32 c = {(float)rk.dt, (float)rk.beta, (float)rk.ab};
+                    float oh, ol;
+                    rk_update_comp(val[k], lo[k], prev[k], prevl[k], r[k], c, use_prev, oh, ol);
+                    outp[k][idx] = oh;
+                    outl[k][idx] = ol;
+                }
+                else {
+                    const RkT64 c = {rk.dt, rk.beta, rk.ab};
+                    double o;
+                    rk_update(val[k], prev[k], r[k], c, use_prev, o);
+                    outp[k][idx] = o;
+                }
             }
         }
         __syncthreads(); /* every thread is done with plane z - 3 and the exchange */
         const int next = z - NGHOST + RING;
         if (tid == 0 && next <= plast) {
             const int s = (next - pfirst) & (RING - 1);
-            mbar_arrive_expect_tx(&bars[s], SLOT_BYTES);
-            tma_load_plane(smem + (size_t)s * SLOT, &tmap, &bars[s], x0, y0, next + NGHOST);
+            mbar_arrive_expect_tx(&bars[s], L::SLOT_BYTES);
+            tma_load_plane(smem + (size_t)s * L::SLOT, &tmap, &bars[s], x0, y0, next + NGHOST);
         }
     }
     if (!ok)
@@ -363,54 +414,87 @@ encode_fn()
     return fn;
 }
 
-} // namespace
-
+template <typename T>
 bool
-ac_tiled_supported(const Geom& g)
-{
-    /* TMA: global strides must be multiples of 16 bytes (mx even) and the box
-     * must not exceed the tensor (nx >= 32, ny >= 4). */
-    return (g.mx % 2) == 0 && g.nx >= TX && g.ny >= TY;
-}
-
-bool
-ac_make_tensor_map64(void* map_out, double* base, const Geom& g)
+make_map(void* map_out, void* base, const Geom& g)
 {
     EncodeTiledFn fn = encode_fn();
-    if (!fn || !ac_tiled_supported(g))
+    if (!fn)
         return false;
     const cuuint64_t dims[4]    = {(cuuint64_t)g.mx, (cuuint64_t)g.my, (cuuint64_t)g.mz,
                                    (cuuint64_t)AC_NF};
-    const cuuint64_t strides[3] = {(cuuint64_t)g.mx * 8, (cuuint64_t)g.mxy * 8,
-                                   (cuuint64_t)g.cells * 8};
-    const cuuint32_t box[4]     = {HX, HY, 1, AC_NF};
+    const cuuint64_t strides[3] = {(cuuint64_t)g.px * sizeof(T), (cuuint64_t)g.pxy * sizeof(T),
+                                   (cuuint64_t)g.cells * sizeof(T)};
+    const cuuint32_t box[4]     = {(cuuint32_t)Tile<T>::HXP, HY, 1, AC_NF};
     const cuuint32_t estr[4]    = {1, 1, 1, 1};
-    const CUresult r = fn((CUtensorMap*)map_out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, base, dims,
-                          strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    const CUresult r = fn((CUtensorMap*)map_out, Tile<T>::kType, 4, base, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
+}
+
+template <typename T, bool COMP>
+cudaError_t
+launch_tiled(const Geom& g, const void* tmap_in, const FieldsT<T>& f, const StencilCoef& sc,
+             const PhysConst& pc, const RkCoef& rk, int* err, cudaStream_t stream,
+             unsigned long long* launches)
+{
+    const dim3 tpb(TX, 2 * TY, 1);
+    const dim3 bpg((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + ZCHUNK - 1) / ZCHUNK);
+    solve_tiled_kernel<T, COMP><<<bpg, tpb, Layout<T>::SMEM_BYTES, stream>>>(
+        *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err);
+    if (launches)
+        ++*launches;
+    return cudaGetLastError();
+}
+
+} // namespace
+
+bool
+ac_tiled_supported(const Geom& g, const int precision)
+{
+    /* TMA: global strides must be multiples of 16 bytes and the box must not
+     * exceed the tensor (mx >= box width, my >= 10). */
+    const int esz = precision == 0 ? 8 : 4;
+    const int hxp = precision == 0 ? Tile<double>::HXP : Tile<float>::HXP;
+    return ((long long)g.px * esz) % 16 == 0 && g.mx >= hxp && g.my >= HY && g.nx >= TX &&
+           g.ny >= TY;
+}
+
+bool
+ac_make_tensor_map(void* map_out, void* base, const Geom& g, const int precision)
+{
+    if (!ac_tiled_supported(g, precision))
+        return false;
+    return precision == 0 ? make_map<double>(map_out, base, g) : make_map<float>(map_out, base, g);
 }
 
 /* Opts the kernel in to its dynamic shared memory on the current device; called
  * by acDeviceCreate, outside any stream capture. */
 cudaError_t
-ac_solve_tiled_init()
+ac_solve_tiled_init(const int precision)
 {
-    return cudaFuncSetAttribute(solve_tiled_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)SMEM_BYTES);
+    if (precision == 0)
+        return cudaFuncSetAttribute(solve_tiled_kernel<double, false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)Layout<double>::SMEM_BYTES);
+    return cudaFuncSetAttribute(solve_tiled_kernel<float, true>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)Layout<float>::SMEM_BYTES);
 }
 
 cudaError_t
-ac_launch_solve64_tiled(const Geom& g, const void* tmap_in, const Fields64& f,
+ac_launch_solve_tiled64(const Geom& g, const void* tmap_in, const Fields64& f,
                         const StencilCoef& sc, const PhysConst& pc, const RkCoef& rk, int* err,
                         cudaStream_t stream, unsigned long long* launches)
 {
-    const dim3 tpb(TX, 2 * TY, 1);
-    const dim3 bpg((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + ZCHUNK - 1) / ZCHUNK);
-    solve_tiled_kernel<<<bpg, tpb, SMEM_BYTES, stream>>>(*(const CUtensorMap*)tmap_in, g, f, sc,
-                                                         pc, rk, err);
-    if (launches)
-        ++*launches;
-    return cudaGetLastError();
+    return launch_tiled<double, false>(g, tmap_in, f, sc, pc, rk, err, stream, launches);
+}
+
+cudaError_t
+ac_launch_solve_tiled32(const Geom& g, const void* tmap_in, const Fields32& f,
+                        const StencilCoef& sc, const PhysConst& pc, const RkCoef& rk, int* err,
+                        cudaStream_t stream, unsigned long long* launches)
+{
+    return launch_tiled<float, true>(g, tmap_in, f, sc, pc, rk, err, stream, launches);
 }

@@ -19,6 +19,10 @@ aa ~ N(0, 1e-4^2)), nu = eta = 5e-3, cs = 1, gamma = 5/3, dt = 1e-3.
               against the measured HBM copy bandwidth.
 * cpu_baseline  the reference's own host model (oracle/_ref) on the host cores,
               a bounded sample (one RK3 step at 96^3), rank 0 at N=1.
+* fp32comp    the same workload with FP32 fields and a compensated FP32 hi/lo RK3
+              state (AC_precision = 1): cell-updates/s, speed-up over FP64, and
+              the per-field relative L-inf against the FP64 path after 100 steps
+              from the same initial mesh (rank 0 at N=1).
 
 --impl reference times that CPU implementation alone, one bounded sample per
 step (rank 0; other ranks exit without work).  Multi-GPU runs are replicas:
@@ -41,7 +45,9 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "cell-updates/s per RK3 step at 512^3 (FP64)"
 UNIT = "cell-updates/s"
-BYTES_PER_CELL_STEP = {"fp64": 512}
+# Minimum HBM bytes per cell per RK3 step: 8 fields x (5 reads + 3 writes) of
+# the state; the FP32-compensated state is a (hi, lo) pair of 4-byte words.
+BYTES_PER_CELL_STEP = {"fp64": 512, "fp32comp": 512}
 REF_SAMPLE_N = 96
 
 
@@ -54,6 +60,8 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp32comp", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=100)
     return ap.parse_args()
 
 
@@ -310,6 +318,10 @@ def run_gpu(args):
                "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": 16,
                "ms_per_step": te * 1e3}
 
+    fp32 = None
+    if world == 1 and not args.no_fp32comp:
+        fp32 = fp32comp_leg(args, ab, torch, host, dev, info)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -336,11 +348,89 @@ def run_gpu(args):
                          "peak_source": peak_kind, "solve_ms_per_step": solve_step_ms,
                          "boundconds_ms_per_step": sum(bc_ms[-3:])},
             "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
+            "fp32comp": fp32,
         }
+        if fp32 and "ms_per_step" in fp32:
+            fp32["speedup_vs_fp64"] = t_max / fp32["ms_per_step"]
         print(json.dumps(line), flush=True)
     dev.destroy()
     if pg:
         pg.destroy_process_group()
+
+
+def timed_steps(dev, torch, stream, steps, dt):
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        dev.integrate_step(dt)
+    e1.record(stream)
+    e1.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def fp32comp_leg(args, ab, torch, host, dev64, info64):
+    """FP32-compensated run of the same workload, and its error against FP64."""
+    import numpy as np
+    n, dt = args.n, 1e-3
+    info = ab.make_info(n, precision=1, **ab.CONFIG_PARAMS)
+    dev = ab.Device(info, device_id=torch.cuda.current_device())
+    stream = torch.cuda.ExternalStream(dev.stream_handle(0))
+    dev.load_mesh(host)
+    for _ in range(args.warmup):
+        dev.integrate_step(dt)
+    dev.synchronize()
+    l0 = dev.launch_count()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms = timed_steps(dev, torch, stream, args.steps, dt)
+    launches = dev.launch_count() - l0
+    solve = []
+    for s in range(3):
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+        dev.periodic_boundconds()
+        e[0].record(stream)
+        dev.integrate_substep(s, dt)
+        e[1].record(stream)
+        dev.swap_buffers()
+        e[1].synchronize()
+        solve.append(e[0].elapsed_time(e[1]))
+    peak, _ = peaks()
+    achieved = BYTES_PER_CELL_STEP["fp32comp"] * n ** 3 / (sum(solve) * 1e-3) / 1e9
+    out = {"value": n ** 3 / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms,
+           "gpu_launches": launches, "clocks": clk.summary(),
+           "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                        "frac": achieved / peak,
+                        "bytes_per_cell_step": BYTES_PER_CELL_STEP["fp32comp"],
+                        "solve_ms_per_step": sum(solve)}}
+    if args.accuracy_steps > 0:
+        # both paths from the same initial mesh, compared field by field
+        dev.load_mesh(host)
+        dev64.load_mesh(host)
+        for _ in range(args.accuracy_steps):
+            dev.integrate_step(dt)
+            dev64.integrate_step(dt)
+        lib = ab.capi.load()
+        C = ab.capi.C
+        shape = ab.empty_mesh(info64).shape[1:]
+        fa = np.zeros(shape)
+        fb = np.zeros(shape)
+        errs = []
+        for q in range(8):
+            # one field at a time: an AcMesh whose only buffer is field q
+            sa, sb = ab.capi.AcMesh(), ab.capi.AcMesh()
+            sa.info, sb.info = info64, info
+            sa.vertex_buffer[q] = fa.ctypes.data_as(C.POINTER(C.c_double))
+            sb.vertex_buffer[q] = fb.ctypes.data_as(C.POINTER(C.c_double))
+            lib.acDeviceStoreVertexBuffer(dev64.handle, 0, q, C.byref(sa))
+            lib.acDeviceStoreVertexBuffer(dev.handle, 0, q, C.byref(sb))
+            ia = fa[3:-3, 3:-3, 3:-3]
+            ib = fb[3:-3, 3:-3, 3:-3]
+            den = float(np.abs(ia).max()) or 1.0
+            errs.append(float(np.abs(ib - ia).max()) / den)
+        out["rel_linf_vs_fp64"] = {"steps": args.accuracy_steps, "per_field": errs,
+                                   "max": max(errs)}
+    dev.destroy()
+    return out
 
 
 def main():
