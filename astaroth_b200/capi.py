@@ -227,7 +227,12 @@ SIGNATURES = {
     "acDeviceGetStreamHandle": (C.c_void_p, [Device_p, C.c_int]),
     "acDeviceGetLaunchCount": (C.c_ulonglong, [Device_p]),
     "acB200Version": (C.c_char_p, []),
+    "acReduceNoAlloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int, C.c_int,
+                                  AcReduction, C.c_void_p, C.c_int, C.c_void_p]),
 }
+
+# acReduceNoAlloc accepts at most this many thread blocks (its static scratch).
+AC_REDUCE_NOALLOC_MAX_BLOCKS = 2048
 
 _lib = None
 

@@ -252,3 +252,111 @@ ac_launch_reduce(const Geom& g, const void* const* fields, const float* const* l
         ++*launches;
     return cudaGetLastError();
 }
+
+/* ------------------------------------------------------------------------
+ * Reduction without any allocation (acReduceNoAlloc).
+ *
+ * For callers that must not allocate device memory: an application or
+ * framework that owns all of the GPU's memory through its own pool or arena
+ * (where a cudaMalloc outside the pool can fail once the pool has reserved the
+ * memory, and where cudaFree would synchronize the whole device), or a coupled
+ * code that runs under a fixed memory budget.  Such a caller keeps its fields
+ * in its own buffers and only wants the reduced value.
+ *
+ * The per-block partials and the block-completion counter of the reduction
+ * kernel above live in this file-scope device array instead of in memory that
+ * acDeviceCreate allocated.  Every GPU that loads the library holds one copy
+ * (33 KB) until the process exits.  The array is shared by all calls on a
+ * device: calls that overlap on the GPU (for example on two streams) race on
+ * it and must be ordered by the caller.
+ * ---------------------------------------------------------------------- */
+namespace {
+
+constexpr int kNoAllocMaxBlocks = AC_REDUCE_NOALLOC_MAX_BLOCKS;
+/* [2 * kNoAllocMaxBlocks partials][counter word] */
+static __device__ __align__(256) double g_noalloc_scratch[2 * kNoAllocMaxBlocks + 32];
+
+constexpr int kMaxDevicesNoAlloc = 64;
+double* g_noalloc_ptr[kMaxDevicesNoAlloc]; /* device address of the array, per device */
+
+} // namespace
+
+extern "C" AcResult
+acReduceNoAlloc(const AcReal* const* fields, const int nfields, const int nx, const int ny,
+                const int nz, const AcReduction reduction, AcReal* result, const int blocks,
+                void* stream)
+{
+    if (!fields || !result || nx <= 0 || ny <= 0 || nz <= 0) {
+        fprintf(stderr, "acReduceNoAlloc: null pointer or empty mesh\n");
+        return AC_FAILURE;
+    }
+    if (nfields != 1 && nfields != 3 && nfields != 4) {
+        fprintf(stderr, "acReduceNoAlloc: nfields must be 1, 3 or 4 (got %d)\n", nfields);
+        return AC_FAILURE;
+    }
+    for (int q = 0; q < nfields; ++q)
+        if (!fields[q]) {
+            fprintf(stderr, "acReduceNoAlloc: fields[%d] is NULL\n", q);
+            return AC_FAILURE;
+        }
+    const int map = nfields == 1 ? reduction.map_vtxbuf_single
+                    : nfields == 3 ? reduction.map_vtxbuf_vec
+                                   : reduction.map_vtxbuf_vec_scal;
+    const bool map_ok = nfields == 1 ? (map >= AC_MAP_VTXBUF && map <= AC_MAP_VTXBUF_EXP_SQUARE)
+                        : nfields == 3 ? (map >= AC_MAP_VTXBUF3_NORM &&
+                                          map <= AC_MAP_VTXBUF3_EXP_SQUARE)
+                                       : (map >= AC_MAP_VTXBUF4_ALFVEN_NORM &&
+                                          map <= AC_MAP_VTXBUF4_ALFVEN_SQUARE);
+    const int op = reduction.reduce_op;
+    if (!map_ok || (op != AC_REDUCE_OP_SUM && op != AC_REDUCE_OP_MAX && op != AC_REDUCE_OP_MIN)) {
+        fprintf(stderr, "acReduceNoAlloc: reduction type does not fit %d field(s)\n", nfields);
+        return AC_FAILURE;
+    }
+
+    Geom g;
+    g.nx    = nx;
+    g.ny    = ny;
+    g.nz    = nz;
+    g.mx    = nx + 2 * NGHOST;
+    g.my    = ny + 2 * NGHOST;
+    g.mz    = nz + 2 * NGHOST;
+    g.px    = g.mx;
+    g.pxy   = (long long)g.px * g.my;
+    g.cells = g.pxy * g.mz;
+
+    const int nb = blocks > 0 ? blocks : ac_reduce_blocks(g);
+    if (nb > kNoAllocMaxBlocks) {
+        fprintf(stderr,
+                "acReduceNoAlloc: %d blocks requested, the static scratch holds at most %d\n",
+                nb, kNoAllocMaxBlocks);
+        return AC_FAILURE;
+    }
+
+    /* One-time set-up per device, on the first call with that device current:
+     * the device address of the scratch array.  In host code the array's name
+     * stands for a host-side shadow, not a device address. */
+    int dev = 0;
+    AC_CUDA_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevicesNoAlloc) {
+        fprintf(stderr, "acReduceNoAlloc: device %d beyond the supported %d\n", dev,
+                kMaxDevicesNoAlloc);
+        return AC_FAILURE;
+    }
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        AC_CUDA_CHECK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+        g_noalloc_ptr[dev] = (double*)p;
+    }
+    double* partials      = g_noalloc_ptr[dev];
+    unsigned int* counter = (unsigned int*)(partials + 2 * kNoAllocMaxBlocks);
+    cudaStream_t st       = (cudaStream_t)stream;
+
+    /* the completion counter must start at zero; the partials need no clearing */
+    AC_CUDA_CHECK(cudaMemsetAsync(counter, 0, sizeof(unsigned int), st));
+    Reader64 f;
+    for (int q = 0; q < 4; ++q)
+        f.p[q] = fields[q < nfields ? q : 0];
+    reduce_kernel<<<nb, kTpb, 0, st>>>(g, f, map, op, partials, counter, result);
+    AC_CUDA_CHECK(cudaGetLastError());
+    return AC_SUCCESS;
+}
