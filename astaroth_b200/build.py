@@ -28,7 +28,7 @@ NVCC_FLAGS = ARCH + [
 ]
 CC_FLAGS = ["-O2", "-fPIC", "-fopenmp", "-std=c11", "-Wall", f"-I{INCLUDE}"]
 
-CU_SOURCES = ["device.cu", "solve.cu", "solve_tiled.cu", "boundconds.cu", "reduce.cu"]
+CU_SOURCES = ["device.cu", "solve.cu", "solve_tiled.cu", "boundconds.cu", "reduce.cu", "cfl.cu"]
 C_SOURCES = ["host.c"]
 HEADERS = ["internal.h", "mhd_rhs.cuh"]
 

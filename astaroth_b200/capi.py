@@ -224,6 +224,10 @@ SIGNATURES = {
                                               C.POINTER(C.POINTER(C.c_double))]),
     "acDeviceMemGetInfo": (C.c_int, [Device_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
     "acDeviceIntegrateStep": (C.c_int, [Device_p, C.c_int, C.c_double]),
+    "acDeviceCalcTimestep": (C.c_int, [Device_p, C.c_int]),
+    "acDeviceGetTimestepMaxima": (C.c_int, [Device_p, C.POINTER(C.c_double),
+                                            C.POINTER(C.c_double)]),
+    "acDeviceGetTimestep": (C.c_int, [Device_p, C.POINTER(C.c_double)]),
     "acDeviceGetStreamHandle": (C.c_void_p, [Device_p, C.c_int]),
     "acDeviceGetLaunchCount": (C.c_ulonglong, [Device_p]),
     "acB200Version": (C.c_char_p, []),

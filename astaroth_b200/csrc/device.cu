@@ -259,12 +259,13 @@ acDeviceCreate(const int id, const AcMeshInfo device_config, Device* device_hand
     /* small scratch block: [partials 2*blocks][result 2][counter, err] */
     const int blocks    = ac_reduce_blocks(d->geom);
     d->red.max_blocks   = blocks;
-    const size_t rbytes = (2 * (size_t)blocks + 2) * sizeof(double) + 64;
+    const size_t rbytes = (2 * (size_t)blocks + 2) * sizeof(double) + 128;
     CREATE_CHECK(cudaMalloc((void**)&d->red.partials, rbytes));
     CREATE_CHECK(cudaMemsetAsync(d->red.partials, 0, rbytes, d->streams[0]));
     d->red.result  = d->red.partials + 2 * (size_t)blocks;
     d->red.counter = (unsigned int*)(d->red.result + 2);
     d->err_flag    = (int*)(d->red.counter + 4);
+    d->cfl         = (unsigned long long*)(d->red.counter + 8);
     d->tmap_ok     = ac_make_tensor_map(&d->tmap[0], d->hi[0], d->geom, precision) &&
                  ac_make_tensor_map(&d->tmap[1], d->hi[1], d->geom, precision);
     if (d->tmap_ok)
@@ -627,16 +628,25 @@ launch_substep(Device d, cudaStream_t st, const int step, const double dt,
     const RkCoef rk = rk_coef(step, dt);
     const int blk   = in_block_index(d);
     const bool tiled = d->solve_variant == 1 && d->tmap_ok && blk >= 0;
+    /* substep 2 also produces the CFL maxima of its input state, as the
+     * reference's calc_timestep inside the third substep (mhdsolver.ac:611) */
+    unsigned long long* cfl = nullptr;
+    if (step == 2) {
+        const cudaError_t e = cudaMemsetAsync(d->cfl, 0, 3 * sizeof(unsigned long long), st);
+        if (e != cudaSuccess)
+            return e;
+        cfl = d->cfl;
+    }
     if (d->precision == 0) {
         const Fields64 f = fields64(d);
         return tiled ? ac_launch_solve_tiled64(d->geom, &d->tmap[blk], f, sc, pc, rk, d->err_flag,
-                                               st, launches)
-                     : ac_launch_solve_plain64(d->geom, f, sc, pc, rk, st, launches);
+                                               cfl, st, launches)
+                     : ac_launch_solve_plain64(d->geom, f, sc, pc, rk, cfl, st, launches);
     }
     const Fields32 f = fields32(d);
-    return tiled ? ac_launch_solve_tiled32(d->geom, &d->tmap[blk], f, sc, pc, rk, d->err_flag, st,
-                                           launches)
-                 : ac_launch_solve_plain32(d->geom, f, sc, pc, rk, st, launches);
+    return tiled ? ac_launch_solve_tiled32(d->geom, &d->tmap[blk], f, sc, pc, rk, d->err_flag, cfl,
+                                           st, launches)
+                 : ac_launch_solve_plain32(d->geom, f, sc, pc, rk, cfl, st, launches);
 }
 
 /* Periodic halo fill of the in-buffer of fields [q0, q0 + nq). */
@@ -898,6 +908,74 @@ acDeviceMemGetInfo(const Device d, size_t* free_mem, size_t* total_mem)
         return AC_FAILURE;
     AC_CUDA_CHECK(cudaSetDevice(d->id));
     AC_CUDA_CHECK(cudaMemGetInfo(free_mem, total_mem));
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceCalcTimestep(const Device d, const Stream stream)
+{
+    if (!d || !stream_ok(stream))
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    StencilCoef sc;
+    ac_make_stencil(d->config, &sc);
+    const double cs2 = d->config.real_params[AC_cs_sound] * d->config.real_params[AC_cs_sound];
+    if (d->precision == 0)
+        AC_CUDA_CHECK(ac_launch_cfl<double>(d->geom, fields64(d), sc, cs2, d->cfl,
+                                            d->streams[stream], &d->launches));
+    else
+        AC_CUDA_CHECK(ac_launch_cfl<float>(d->geom, fields32(d), sc, cs2, d->cfl,
+                                           d->streams[stream], &d->launches));
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceGetTimestepMaxima(const Device d, AcReal* uu_max, AcReal* alfven_max)
+{
+    if (!d || !uu_max || !alfven_max)
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    for (int s = 0; s < NUM_STREAMS; ++s)
+        AC_CUDA_CHECK(cudaStreamSynchronize(d->streams[s]));
+    unsigned long long w[3];
+    AC_CUDA_CHECK(cudaMemcpy(w, d->cfl, sizeof(w), cudaMemcpyDeviceToHost));
+    double v[3];
+    memcpy(v, w, sizeof(v));
+    *uu_max     = v[0];
+    *alfven_max = v[1];
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceGetTimestep(const Device d, AcReal* dt)
+{
+    if (!d || !dt)
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    for (int s = 0; s < NUM_STREAMS; ++s)
+        AC_CUDA_CHECK(cudaStreamSynchronize(d->streams[s]));
+    unsigned long long w[3];
+    AC_CUDA_CHECK(cudaMemcpy(w, d->cfl, sizeof(w), cudaMemcpyDeviceToHost));
+    double v[3];
+    memcpy(v, w, sizeof(v));
+    if (d->config.int_params[AC_additive_timestep]) {
+        /* mhdsolver.ac:558-569: min over cells of min(visc_dt, advec_dt); visc_dt is
+         * uniform, so the minimum of advec_dt comes from the maximum of
+         * |u| + sqrt(cs^2 + vA^2) */
+        const AcMeshInfo& c = d->config;
+        const double dsmin  = c.real_params[AC_dsmin];
+        double visc         = c.real_params[AC_nu_visc] > c.real_params[AC_eta]
+                                  ? c.real_params[AC_nu_visc]
+                                  : c.real_params[AC_eta];
+        const double gchi   = c.real_params[AC_gamma] * c.real_params[AC_chi];
+        visc                = visc > gchi ? visc : gchi;
+        const double visc_dt  = visc > 0 ? c.real_params[AC_cdtv] * dsmin * dsmin / visc : INFINITY;
+        const double advec_dt = c.real_params[AC_cdt] * dsmin / v[2];
+        *dt                   = visc_dt < advec_dt ? visc_dt : advec_dt;
+    }
+    else {
+        *dt = acHostTimestepFromMaxima(d->config, v[0], v[1]);
+    }
     return AC_SUCCESS;
 }
 

@@ -128,6 +128,9 @@ struct device_s {
     CUtensorMap tmap[2]; /* 4-D (x, y, z, field) maps of the value (hi) array of each block */
     int tmap_ok;
     int* err_flag;       /* device word set by kernels whose bounded waits gave up */
+    /* CFL maxima of the last substep 2 (bit patterns of non-negative doubles):
+     * [0] max |u|, [1] max Alfven speed |B|/sqrt(rho), [2] max |u| + sqrt(cs^2 + vA^2) */
+    unsigned long long* cfl;
     int id;
     AcMeshInfo config;
     Geom geom;
@@ -164,10 +167,12 @@ cudaError_t ac_launch_join(const Geom& g, const float* hi, const float* lo, doub
                            cudaStream_t stream, unsigned long long* launches);
 
 cudaError_t ac_launch_solve_plain64(const Geom& g, const Fields64& f, const StencilCoef& sc,
-                                    const PhysConst& pc, const RkCoef& rk, cudaStream_t stream,
+                                    const PhysConst& pc, const RkCoef& rk,
+                                    unsigned long long* cfl, cudaStream_t stream,
                                     unsigned long long* launches);
 cudaError_t ac_launch_solve_plain32(const Geom& g, const Fields32& f, const StencilCoef& sc,
-                                    const PhysConst& pc, const RkCoef& rk, cudaStream_t stream,
+                                    const PhysConst& pc, const RkCoef& rk,
+                                    unsigned long long* cfl, cudaStream_t stream,
                                     unsigned long long* launches);
 
 /* map: AcKernel of the reduction's map; op: AcReduceOp; up to 4 fields; lo
@@ -184,10 +189,18 @@ bool ac_make_tensor_map(void* map_out, void* base, const Geom& g, const int prec
 cudaError_t ac_solve_tiled_init(const int precision);
 cudaError_t ac_launch_solve_tiled64(const Geom& g, const void* tmap_in, const Fields64& f,
                                     const StencilCoef& sc, const PhysConst& pc, const RkCoef& rk,
-                                    int* err, cudaStream_t stream, unsigned long long* launches);
+                                    int* err, unsigned long long* cfl, cudaStream_t stream,
+                                    unsigned long long* launches);
 cudaError_t ac_launch_solve_tiled32(const Geom& g, const void* tmap_in, const Fields32& f,
                                     const StencilCoef& sc, const PhysConst& pc, const RkCoef& rk,
-                                    int* err, cudaStream_t stream, unsigned long long* launches);
+                                    int* err, unsigned long long* cfl, cudaStream_t stream,
+                                    unsigned long long* launches);
+
+/* CFL maxima of the in-buffer (cfl.cu); zeroes the three words first. */
+template <typename T>
+cudaError_t ac_launch_cfl(const Geom& g, const FieldsT<T>& f, const StencilCoef& sc,
+                          const double cs2_sound, unsigned long long* cfl, cudaStream_t stream,
+                          unsigned long long* launches);
 
 /* Host-side setup helpers (device.cu). */
 void ac_make_stencil(const AcMeshInfo& info, StencilCoef* sc);

@@ -286,3 +286,47 @@ rk_update_comp(const float h, const float l, const float ph, const float pl, con
     oh             = __fadd_rn(s, l2);
     ol             = __fsub_rn(l2, __fsub_rn(oh, s));
 }
+
+/* Per-cell quantities of calc_timestep (acc-runtime/samples/mhd_modular/mhdsolver.ac:551-583):
+ * |u|, the Alfven speed sqrt(|B|^2 / rho) and |u| + sqrt(cs_sound^2 + vA^2), folded into
+ * running maxima m[3]. */
+template <typename T>
+__device__ __forceinline__ void
+cfl_accumulate(const T u2, const T b2, const T inv_rho, const T cs2_sound, T m[3])
+{
+    const T va2  = b2 * inv_rho;
+    const T umag = sqrt(u2);
+    m[0]         = fmax(m[0], umag);
+    m[1]         = fmax(m[1], sqrt(va2));
+    m[2]         = fmax(m[2], umag + sqrt(cs2_sound + va2));
+}
+
+/* Block-wide max of m[3] across all threads, then one atomicMax per value on
+ * the device words (non-negative doubles order like their bit patterns).
+ * Every thread of the block must call this; red holds 3 * warps entries. */
+template <typename T>
+__device__ __forceinline__ void
+cfl_commit(T m[3], T* red, unsigned long long* cfl)
+{
+    const int lane = threadIdx.x & 31;
+    const int nthreads = blockDim.x * blockDim.y;
+    const int tid      = threadIdx.y * blockDim.x + threadIdx.x;
+    const int warp     = tid >> 5;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+            m[i] = fmax(m[i], __shfl_xor_sync(0xffffffffu, m[i], o));
+    if (lane == 0)
+        for (int i = 0; i < 3; ++i)
+            red[3 * warp + i] = m[i];
+    __syncthreads();
+    if (tid == 0) {
+        for (int i = 0; i < 3; ++i) {
+            T v = red[i];
+            for (int w = 1; w < nthreads / 32; ++w)
+                v = fmax(v, red[3 * w + i]);
+            atomicMax(cfl + i, (unsigned long long)__double_as_longlong((double)v));
+        }
+    }
+}

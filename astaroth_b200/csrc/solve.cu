@@ -110,13 +110,18 @@ vec_derivs(const T* const* fc, const long long* st, const StencilT<T>& sc, VecD<
 template <typename T, bool COMP>
 __global__ void __launch_bounds__(128)
 solve_plain_kernel(const Geom g, const FieldsT<T> f, const StencilT<T> sc, const PhysConst pc,
-                   const RkCoef rk)
+                   const RkCoef rk, unsigned long long* cfl)
 {
+    __shared__ T red[3 * 4];
     const int i = threadIdx.x + blockIdx.x * blockDim.x;
     const int j = threadIdx.y + blockIdx.y * blockDim.y;
     const int k = blockIdx.z;
-    if (i >= g.nx || j >= g.ny || k >= g.nz)
+    T cm[3]     = {0, 0, 0};
+    if (i >= g.nx || j >= g.ny || k >= g.nz) {
+        if (cfl)
+            cfl_commit(cm, red, cfl); /* every thread of the block takes part */
         return;
+    }
     const long long idx   = geom_idx(g, i + NGHOST, j + NGHOST, k + NGHOST);
     const long long st[3] = {1, (long long)g.px, g.pxy};
     const bool use_prev   = rk.step > 0;
@@ -145,6 +150,12 @@ solve_plain_kernel(const Geom g, const FieldsT<T> f, const StencilT<T> sc, const
     T r[AC_NF];
     mhd_rates(L, S, U, A, p, r);
 
+    if (cfl) {
+        const T Bx = A.g[2][1] - A.g[1][2], By = A.g[0][2] - A.g[2][0], Bz = A.g[1][0] - A.g[0][1];
+        cfl_accumulate(U.v[0] * U.v[0] + U.v[1] * U.v[1] + U.v[2] * U.v[2],
+                       Bx * Bx + By * By + Bz * Bz, ac_exp(-L.v), p.cs2_sound, cm);
+    }
+
     const T val[AC_NF] = {L.v, U.v[0], U.v[1], U.v[2], A.v[0], A.v[1], A.v[2], S.v};
 #pragma unroll
     for (int q = 0; q < AC_NF; ++q) {
@@ -162,16 +173,19 @@ solve_plain_kernel(const Geom g, const FieldsT<T> f, const StencilT<T> sc, const
             f.out[q][idx] = o;
         }
     }
+    if (cfl)
+        cfl_commit(cm, red, cfl);
 }
 
 template <typename T, bool COMP>
 cudaError_t
 launch_plain(const Geom& g, const FieldsT<T>& f, const StencilCoef& sc, const PhysConst& pc,
-             const RkCoef& rk, cudaStream_t stream, unsigned long long* launches)
+             const RkCoef& rk, unsigned long long* cfl, cudaStream_t stream,
+             unsigned long long* launches)
 {
     const dim3 tpb(32, 4, 1);
     const dim3 bpg((g.nx + tpb.x - 1) / tpb.x, (g.ny + tpb.y - 1) / tpb.y, g.nz);
-    solve_plain_kernel<T, COMP><<<bpg, tpb, 0, stream>>>(g, f, stencil_cast<T>(sc), pc, rk);
+    solve_plain_kernel<T, COMP><<<bpg, tpb, 0, stream>>>(g, f, stencil_cast<T>(sc), pc, rk, cfl);
     if (launches)
         ++*launches;
     return cudaGetLastError();
@@ -181,16 +195,16 @@ launch_plain(const Geom& g, const FieldsT<T>& f, const StencilCoef& sc, const Ph
 
 cudaError_t
 ac_launch_solve_plain64(const Geom& g, const Fields64& f, const StencilCoef& sc,
-                        const PhysConst& pc, const RkCoef& rk, cudaStream_t stream,
-                        unsigned long long* launches)
+                        const PhysConst& pc, const RkCoef& rk, unsigned long long* cfl,
+                        cudaStream_t stream, unsigned long long* launches)
 {
-    return launch_plain<double, false>(g, f, sc, pc, rk, stream, launches);
+    return launch_plain<double, false>(g, f, sc, pc, rk, cfl, stream, launches);
 }
 
 cudaError_t
 ac_launch_solve_plain32(const Geom& g, const Fields32& f, const StencilCoef& sc,
-                        const PhysConst& pc, const RkCoef& rk, cudaStream_t stream,
-                        unsigned long long* launches)
+                        const PhysConst& pc, const RkCoef& rk, unsigned long long* cfl,
+                        cudaStream_t stream, unsigned long long* launches)
 {
-    return launch_plain<float, true>(g, f, sc, pc, rk, stream, launches);
+    return launch_plain<float, true>(g, f, sc, pc, rk, cfl, stream, launches);
 }

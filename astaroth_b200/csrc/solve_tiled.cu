@@ -232,7 +232,8 @@ vec_derivs(const Taps<T>& t, const int q0, const StencilT<T>& sc, VecD<T>& o)
 template <typename T, bool COMP>
 __global__ void __launch_bounds__(2 * TX * TY, Tile<T>::MINB)
 solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const FieldsT<T> f,
-                   const StencilT<T> sc, const PhysConst pc, const RkCoef rk, int* err)
+                   const StencilT<T> sc, const PhysConst pc, const RkCoef rk, int* err,
+                   unsigned long long* cfl)
 {
     typedef Layout<T> L;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -286,6 +287,7 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
     }
     bool ok    = true;
     int waited = pfirst - 1;
+    T cm[3]    = {0, 0, 0}; /* CFL maxima of this thread (substep 2 only) */
 
     for (int z = z0; z < z1; ++z) {
         const long long idx = geom_idx(g, x + NGHOST, y + NGHOST, z + NGHOST);
@@ -359,6 +361,13 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
                 for (int k = 0; k < AC_H2M_COUNT; ++k)
                     hx.a[k] = xh[k * NCELL + cell];
                 mag_rates(sd, vd, mx, hx, p, r);
+                if (cfl) {
+                    const T* u = &hx.a[H2M_U];
+                    const T* B = &mx.a[M2H_B];
+                    cfl_accumulate(u[0] * u[0] + u[1] * u[1] + u[2] * u[2],
+                                   B[0] * B[0] + B[1] * B[1] + B[2] * B[2], hx.a[H2M_INV_RHO],
+                                   p.cs2_sound, cm);
+                }
                 val[0] = vd.v[0];
                 val[1] = vd.v[1];
                 val[2] = vd.v[2];
@@ -390,6 +399,8 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
             tma_load_plane(smem + (size_t)s * L::SLOT, &tmap, &bars[s], x0, y0, next + NGHOST);
         }
     }
+    if (cfl)
+        cfl_commit(cm, xh, cfl); /* the exchange area is free after the last barrier */
     if (!ok)
         atomicExch(err, 1);
 }
@@ -436,13 +447,13 @@ make_map(void* map_out, void* base, const Geom& g)
 template <typename T, bool COMP>
 cudaError_t
 launch_tiled(const Geom& g, const void* tmap_in, const FieldsT<T>& f, const StencilCoef& sc,
-             const PhysConst& pc, const RkCoef& rk, int* err, cudaStream_t stream,
-             unsigned long long* launches)
+             const PhysConst& pc, const RkCoef& rk, int* err, unsigned long long* cfl,
+             cudaStream_t stream, unsigned long long* launches)
 {
     const dim3 tpb(TX, 2 * TY, 1);
     const dim3 bpg((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + ZCHUNK - 1) / ZCHUNK);
     solve_tiled_kernel<T, COMP><<<bpg, tpb, Layout<T>::SMEM_BYTES, stream>>>(
-        *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err);
+        *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err, cfl);
     if (launches)
         ++*launches;
     return cudaGetLastError();
@@ -486,15 +497,17 @@ ac_solve_tiled_init(const int precision)
 cudaError_t
 ac_launch_solve_tiled64(const Geom& g, const void* tmap_in, const Fields64& f,
                         const StencilCoef& sc, const PhysConst& pc, const RkCoef& rk, int* err,
-                        cudaStream_t stream, unsigned long long* launches)
+                        unsigned long long* cfl, cudaStream_t stream,
+                        unsigned long long* launches)
 {
-    return launch_tiled<double, false>(g, tmap_in, f, sc, pc, rk, err, stream, launches);
+    return launch_tiled<double, false>(g, tmap_in, f, sc, pc, rk, err, cfl, stream, launches);
 }
 
 cudaError_t
 ac_launch_solve_tiled32(const Geom& g, const void* tmap_in, const Fields32& f,
                         const StencilCoef& sc, const PhysConst& pc, const RkCoef& rk, int* err,
-                        cudaStream_t stream, unsigned long long* launches)
+                        unsigned long long* cfl, cudaStream_t stream,
+                        unsigned long long* launches)
 {
-    return launch_tiled<float, true>(g, tmap_in, f, sc, pc, rk, err, stream, launches);
+    return launch_tiled<float, true>(g, tmap_in, f, sc, pc, rk, err, cfl, stream, launches);
 }

@@ -226,6 +226,21 @@ class Device:
                "acDeviceReduceVecScal")
         return out.value
 
+    # ---- CFL timestep (computed by substep 2, or by calc_timestep) ----
+    def calc_timestep(self, stream: int = 0) -> None:
+        _check(self.lib.acDeviceCalcTimestep(self._h, stream), "acDeviceCalcTimestep")
+
+    def timestep_maxima(self):
+        u, va = C.c_double(), C.c_double()
+        _check(self.lib.acDeviceGetTimestepMaxima(self._h, C.byref(u), C.byref(va)),
+               "acDeviceGetTimestepMaxima")
+        return u.value, va.value
+
+    def timestep(self) -> float:
+        dt = C.c_double()
+        _check(self.lib.acDeviceGetTimestep(self._h, C.byref(dt)), "acDeviceGetTimestep")
+        return dt.value
+
     # ---- introspection ----
     def stream_handle(self, stream: int = 0) -> int:
         return self.lib.acDeviceGetStreamHandle(self._h, stream) or 0

@@ -317,3 +317,80 @@ def test_two_devices_on_one_gpu_are_independent():
         a, b = d1.store_mesh(), d2.store_mesh()
     assert np.array_equal(oracle.interior(a), oracle.interior(gpu_run(info, f1, 1e-3, 1)))
     assert np.array_equal(oracle.interior(b), oracle.interior(gpu_run(info, f2, 1e-3, 1)))
+
+
+# ---------------------------------------------------------------- CFL timestep
+
+def _d1(f, axis, ds):
+    c = (3 / 4, -3 / 20, 1 / 60)
+    return sum(ck * (np.roll(f, -k, axis) - np.roll(f, k, axis))
+               for k, ck in zip((1, 2, 3), c)) / ds
+
+
+def numpy_cfl(f, info):
+    """max |u|, max |curl A|/sqrt(rho), max |u| + sqrt(cs^2 + vA^2) on the periodic interior."""
+    p = ab.info_to_dict(info)
+    q = oracle.interior(f)
+    ds = p["ds"]
+    grad = lambda g: [_d1(g, 2, ds[0]), _d1(g, 1, ds[1]), _d1(g, 0, ds[2])]  # noqa: E731
+    ga = [grad(q[4 + c]) for c in range(3)]
+    B = [ga[2][1] - ga[1][2], ga[0][2] - ga[2][0], ga[1][0] - ga[0][1]]
+    b2 = B[0] ** 2 + B[1] ** 2 + B[2] ** 2
+    va2 = b2 / np.exp(q[0])
+    umag = np.sqrt(q[1] ** 2 + q[2] ** 2 + q[3] ** 2)
+    return umag.max(), np.sqrt(va2).max(), (umag + np.sqrt(p["cs_sound"] ** 2 + va2)).max()
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-13), (1, 1e-5)])
+def test_cfl_maxima_and_timestep(precision, tol):
+    info = ab.make_info((48, 32, 24), precision=precision, **ab.CONFIG_PARAMS)
+    f = ab.seeded_mesh(info, 14, amp_scalar=0.05, sigma_uu=0.05, sigma_aa=0.02)
+    oracle.periodic_bounds(f, "port")
+    want_u, want_va, _ = numpy_cfl(f, info)
+    with ab.Device(info) as dev:
+        dev.load_mesh(f)
+        dev.calc_timestep()
+        u, va = dev.timestep_maxima()
+        assert abs(u - want_u) <= tol * want_u and abs(va - want_va) <= tol * want_va
+        dt = dev.timestep()
+        assert dt == ab.timestep_from_maxima(info, u, va)
+        # substep 2 computes the same maxima from its input state on the fly
+        dev.integrate_substep(2, 1e-3)
+        u2, va2 = dev.timestep_maxima()
+        assert abs(u2 - want_u) <= tol * want_u and abs(va2 - want_va) <= tol * want_va
+
+
+def test_additive_timestep():
+    info = ab.make_info(32, **ab.CONFIG_PARAMS)
+    info.int_params[ab.capi.IntParam.AC_additive_timestep] = 1
+    f = ab.seeded_mesh(info, 15, amp_scalar=0.05, sigma_uu=0.05, sigma_aa=0.02)
+    oracle.periodic_bounds(f, "port")
+    _, _, want_adv = numpy_cfl(f, info)
+    p = ab.info_to_dict(info)
+    ds = p["ds"][0]
+    chi = info.real_params[ab.capi.RealParam.AC_chi]
+    visc = max(p["nu_visc"], p["eta"], p["gamma"] * chi)
+    want = min(0.3 * ds * ds / visc, 0.4 * ds / want_adv)
+    with ab.Device(info) as dev:
+        dev.load_mesh(f)
+        dev.calc_timestep()
+        assert dev.timestep() == pytest.approx(want, rel=1e-13)
+
+
+def test_adaptive_run_is_stable():
+    """Config 2 in miniature: solenoidal modes, FP32-comp, CFL-adaptive dt."""
+    info = ab.make_info(64, precision=1, **ab.CONFIG_PARAMS)
+    f = ab.seeded_mesh(info, 3)
+    ab.solenoidal_velocity(f, info, seed=3, nmodes=64, kmax=8, amplitude=1e-2)
+    with ab.Device(info) as dev:
+        dev.load_mesh(f)
+        dev.periodic_boundconds()
+        dev.calc_timestep()
+        dts = []
+        for _ in range(5):
+            dt = dev.timestep()
+            dts.append(dt)
+            dev.integrate_step(dt)
+        out = dev.store_mesh()
+    assert all(np.isfinite(dts)) and min(dts) > 0
+    assert np.all(np.isfinite(oracle.interior(out)))
