@@ -107,21 +107,12 @@ vec_derivs(const T* const* fc, const long long* st, const StencilT<T>& sc, VecD<
     o.gd[2]       = mxz_x + myz_y + diag[2];
 }
 
+/* One cell of the plain kernel; adds the cell's CFL quantities to cm when cfl is set. */
 template <typename T, bool COMP>
-__global__ void __launch_bounds__(128)
-solve_plain_kernel(const Geom g, const FieldsT<T> f, const StencilT<T> sc, const PhysConst pc,
-                   const RkCoef rk, unsigned long long* cfl)
+__device__ __forceinline__ void
+plain_cell(const Geom& g, const FieldsT<T>& f, const StencilT<T>& sc, const PhysConst& pc,
+           const RkCoef& rk, const bool cfl, const int i, const int j, const int k, T cm[3])
 {
-    __shared__ T red[3 * 4];
-    const int i = threadIdx.x + blockIdx.x * blockDim.x;
-    const int j = threadIdx.y + blockIdx.y * blockDim.y;
-    const int k = blockIdx.z;
-    T cm[3]     = {0, 0, 0};
-    if (i >= g.nx || j >= g.ny || k >= g.nz) {
-        if (cfl)
-            cfl_commit(cm, red, cfl); /* every thread of the block takes part */
-        return;
-    }
     const long long idx   = geom_idx(g, i + NGHOST, j + NGHOST, k + NGHOST);
     const long long st[3] = {1, (long long)g.px, g.pxy};
     const bool use_prev   = rk.step > 0;
@@ -173,6 +164,22 @@ solve_plain_kernel(const Geom g, const FieldsT<T> f, const StencilT<T> sc, const
             f.out[q][idx] = o;
         }
     }
+}
+
+/* Every thread reaches the single cfl_commit at the end (it uses full-warp
+ * shuffles and a block barrier), so there is no early return. */
+template <typename T, bool COMP>
+__global__ void __launch_bounds__(128)
+solve_plain_kernel(const Geom g, const FieldsT<T> f, const StencilT<T> sc, const PhysConst pc,
+                   const RkCoef rk, unsigned long long* cfl)
+{
+    __shared__ T red[3 * 4];
+    const int i = threadIdx.x + blockIdx.x * blockDim.x;
+    const int j = threadIdx.y + blockIdx.y * blockDim.y;
+    const int k = blockIdx.z;
+    T cm[3]     = {0, 0, 0};
+    if (i < g.nx && j < g.ny && k < g.nz)
+        plain_cell<T, COMP>(g, f, sc, pc, rk, cfl != nullptr, i, j, k, cm);
     if (cfl)
         cfl_commit(cm, red, cfl);
 }
