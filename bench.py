@@ -213,16 +213,11 @@ def run_gpu(args):
 
     import astaroth_b200 as ab
     from astaroth_b200 import capi
+    from astaroth_b200 import dist as adist
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-        pg = dist
+    adist.init("nccl")
 
     n = args.n
     info = ab.make_info(n, **ab.CONFIG_PARAMS)
@@ -233,9 +228,7 @@ def run_gpu(args):
     dev.synchronize()
     stream = torch.cuda.ExternalStream(dev.stream_handle(0), device=torch.device("cuda", local))
 
-    def barrier():
-        if pg:
-            pg.barrier()
+    barrier = adist.barrier
 
     for _ in range(args.warmup):
         dev.integrate_step(dt)
@@ -257,11 +250,7 @@ def run_gpu(args):
     barrier()
     launches = dev.launch_count() - launches0
     t_ms = ev0.elapsed_time(ev1) / args.steps
-    t_max = t_ms
-    if pg:
-        t = torch.tensor([t_ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        t_max = float(t.item())
+    t_max = adist.max_over_ranks(t_ms)
     clocks = clk.summary()
 
     # ---- per-kernel times of the solve kernel (same stream, plain launches)
@@ -309,11 +298,7 @@ def run_gpu(args):
         ke = max(2, min(args.steps, 5))
         for _ in range(ke):
             e2e_step()
-        te = (time.perf_counter() - t0) / ke
-        if pg:
-            t = torch.tensor([te], device="cuda")
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            te = float(t.item())
+        te = adist.max_over_ranks((time.perf_counter() - t0) / ke)
         e2e = {"value": world * cells / te, "unit": UNIT,
                "h2d_bytes_per_step": int(host.nbytes), "d2h_bytes_per_step": 16,
                "ms_per_step": te * 1e3}
@@ -354,8 +339,8 @@ def run_gpu(args):
             fp32["speedup_vs_fp64"] = t_max / fp32["ms_per_step"]
         print(json.dumps(line), flush=True)
     dev.destroy()
-    if pg:
-        pg.destroy_process_group()
+    adist.barrier()
+    adist.destroy()
 
 
 def timed_steps(dev, torch, stream, steps, dt):
