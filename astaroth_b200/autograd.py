@@ -1,0 +1,128 @@
+"""torch.autograd over the C ABI: the MHD time integration as a differentiable
+function of the initial fields and of nu, eta.
+
+Forward: N RK3 steps of the device integrator (acDeviceIntegrateStep), with a
+checkpoint of the state every k steps.  Backward: for each checkpoint segment,
+from the last to the first, the states at the start of its steps are
+recomputed, and for each step (last first) the substep states f_0, f_1, f_2
+are recomputed and the discrete adjoint substeps s = 2, 1, 0 are applied
+(acDeviceIntegrateSubstepAdjoint).  Memory: the checkpoints, one segment of
+step states and three substep states, so O(N/k + k) meshes instead of O(N).
+
+Tensors are (8, mz, my, mx) float64 on the GPU (halos included, as the host
+AcMesh).  The integration fills the halos itself, so gradients live on the
+interior; the returned gradient is zero on the halo cells.
+"""
+from __future__ import annotations
+
+import math
+
+import torch
+
+from . import capi
+from .device import Device
+
+D1 = (3 / 4, -3 / 20, 1 / 60)
+
+
+def interior(t):
+    return t[..., 3:-3, 3:-3, 3:-3]
+
+
+def _d1(f, axis, inv_ds):
+    """6th-order first derivative of periodic interior data along a tensor axis."""
+    out = torch.zeros_like(f)
+    for k, c in zip((1, 2, 3), D1):
+        out = out + c * (torch.roll(f, -k, axis) - torch.roll(f, k, axis))
+    return out * inv_ds
+
+
+def energy(fields: torch.Tensor, info) -> torch.Tensor:
+    """J = sum over the interior of (1/2) exp(lnrho) |u|^2 dV + |curl A|^2 / (2 mu0) dV,
+    with the same 6th-order first derivatives as the solver (periodic box)."""
+    q = interior(fields)
+    ds = info.real3_params[capi.Real3Param.AC_ds]
+    inv = (1.0 / ds.x, 1.0 / ds.y, 1.0 / ds.z)
+    dV = ds.x * ds.y * ds.z
+    mu0 = info.real_params[capi.RealParam.AC_mu0]
+    lnrho, u, a = q[0], q[1:4], q[4:7]
+    ekin = 0.5 * (torch.exp(lnrho) * (u * u).sum(0)).sum() * dV
+    # axes of a field: (z, y, x) -> x = 2, y = 1, z = 0
+    g = [[_d1(a[c], 2, inv[0]), _d1(a[c], 1, inv[1]), _d1(a[c], 0, inv[2])] for c in range(3)]
+    bx = g[2][1] - g[1][2]
+    by = g[0][2] - g[2][0]
+    bz = g[1][0] - g[0][1]
+    emag = ((bx * bx + by * by + bz * bz).sum() / (2.0 * mu0)) * dV
+    return ekin + emag
+
+
+class _Integrate(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, f0, nu, eta, dev, steps, dt, every):
+        dev.set_real(capi.RealParam.AC_nu_visc, float(nu))
+        dev.set_real(capi.RealParam.AC_eta, float(eta))
+        dev.load_mesh_device(f0.contiguous())
+        ckpts = [f0.detach().clone()]
+        for n in range(steps):
+            dev.integrate_step(dt)
+            if (n + 1) % every == 0 and n + 1 < steps:
+                ckpts.append(dev.store_mesh_device(torch.empty_like(f0)))
+        out = dev.store_mesh_device(torch.empty_like(f0))
+        torch.cuda.synchronize()
+        ctx.dev, ctx.steps, ctx.dt, ctx.every, ctx.ckpts = dev, steps, dt, every, ckpts
+        ctx.nu, ctx.eta = float(nu), float(eta)
+        return out
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        dev, steps, dt, every = ctx.dev, ctx.steps, ctx.dt, ctx.every
+        dev.set_real(capi.RealParam.AC_nu_visc, ctx.nu)
+        dev.set_real(capi.RealParam.AC_eta, ctx.eta)
+        lam = torch.zeros_like(grad_out)
+        interior(lam).copy_(interior(grad_out))
+        dev.load_adjoint(lam.contiguous())
+        nseg = len(ctx.ckpts)
+        for seg in reversed(range(nseg)):
+            n0 = seg * every
+            n1 = min(n0 + every, steps)
+            # states at the start of the segment's steps
+            states = [ctx.ckpts[seg]]
+            dev.load_mesh_device(ctx.ckpts[seg])
+            for _ in range(n0, n1 - 1):
+                dev.integrate_step(dt)
+                states.append(dev.store_mesh_device(torch.empty_like(grad_out)))
+            for n in reversed(range(n1 - n0)):
+                # substep states f_0, f_1, f_2 of this step
+                sub = [states[n]]
+                dev.load_mesh_device(states[n])
+                for s in (0, 1):
+                    dev.periodic_boundconds()
+                    dev.integrate_substep(s, dt)
+                    dev.swap_buffers()
+                    sub.append(dev.store_mesh_device(torch.empty_like(grad_out)))
+                for s in (2, 1, 0):
+                    dev.load_mesh_device(sub[s])
+                    dev.periodic_boundconds()
+                    dev.integrate_substep_adjoint(s, dt)
+        g0 = torch.zeros_like(grad_out)
+        dev.store_adjoint(g0)
+        torch.cuda.synchronize()
+        out = torch.zeros_like(g0)
+        interior(out).copy_(interior(g0))
+        nu_bar, eta_bar = dev.param_adjoints()
+        dtype, device = grad_out.dtype, grad_out.device
+        return (out, torch.tensor(nu_bar, dtype=dtype, device=device),
+                torch.tensor(eta_bar, dtype=dtype, device=device), None, None, None, None)
+
+
+def integrate(f0: torch.Tensor, nu, eta, dev: Device, steps: int, dt: float,
+              checkpoint_every: int | None = None) -> torch.Tensor:
+    """Differentiable N-step integration on `dev` (an FP64 Device of matching size).
+
+    f0: (8, mz, my, mx) float64 CUDA tensor; nu, eta: 0-d tensors (may require grad).
+    Returns the final state; backward gives d/d f0 (interior), d/d nu and d/d eta.
+    """
+    every = checkpoint_every or max(1, int(math.sqrt(steps)))
+    nu = torch.as_tensor(nu, dtype=torch.float64, device=f0.device)
+    eta = torch.as_tensor(eta, dtype=torch.float64, device=f0.device)
+    return _Integrate.apply(f0, nu, eta, dev, steps, dt, every)

@@ -228,6 +228,14 @@ SIGNATURES = {
     "acDeviceGetTimestepMaxima": (C.c_int, [Device_p, C.POINTER(C.c_double),
                                             C.POINTER(C.c_double)]),
     "acDeviceGetTimestep": (C.c_int, [Device_p, C.POINTER(C.c_double)]),
+    "acDeviceLoadMeshDevice": (C.c_int, [Device_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "acDeviceStoreMeshDevice": (C.c_int, [Device_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "acDeviceLoadAdjoint": (C.c_int, [Device_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "acDeviceIntegrateSubstepAdjoint": (C.c_int, [Device_p, C.c_int, C.c_int, Volume, Volume,
+                                                  C.c_double]),
+    "acDeviceStoreAdjoint": (C.c_int, [Device_p, C.c_int, C.POINTER(C.c_void_p)]),
+    "acDeviceGetParamAdjoints": (C.c_int, [Device_p, C.POINTER(C.c_double),
+                                           C.POINTER(C.c_double)]),
     "acDeviceGetStreamHandle": (C.c_void_p, [Device_p, C.c_int]),
     "acDeviceGetLaunchCount": (C.c_ulonglong, [Device_p]),
     "acB200Version": (C.c_char_p, []),

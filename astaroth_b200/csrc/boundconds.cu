@@ -20,7 +20,9 @@
 
 namespace {
 
-constexpr int kMaxArrays = 2 * AC_NF; /* FP32 compensated: hi and lo of 8 fields */
+/* FP32 compensated meshes fill hi and lo of 8 fields (16 arrays); the adjoint
+ * fills its 46 derivative-slot arrays. */
+constexpr int kMaxArrays = 48;
 
 template <typename T>
 struct ArrayList {

@@ -173,6 +173,10 @@ release(Device d)
     }
     cudaFree(d->staging);
     cudaFree(d->red.partials);
+    cudaFree(d->adj_lf);
+    cudaFree(d->adj_lw);
+    cudaFree(d->adj_mu);
+    cudaFree(d->adj_pgrad);
     cudaFreeHost(d->host_result);
     for (int s = 0; s < NUM_STREAMS; ++s)
         if (d->streams[s])
@@ -976,6 +980,152 @@ acDeviceGetTimestep(const Device d, AcReal* dt)
     else {
         *dt = acHostTimestepFromMaxima(d->config, v[0], v[1]);
     }
+    return AC_SUCCESS;
+}
+
+/* ---- transfers from and to caller-owned device arrays ---- */
+
+extern "C" AcResult
+acDeviceLoadMeshDevice(const Device d, const Stream stream, const AcReal* const* src)
+{
+    if (!d || !src || !stream_ok(stream))
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    const size_t n = (size_t)d->geom.mx * d->geom.my * d->geom.mz;
+    for (int q = 0; q < AC_NF; ++q) {
+        if (!src[q])
+            return AC_NOT_ALLOCATED;
+        const int b = d->in_idx[q];
+        if (d->precision == 0)
+            AC_CUDA_CHECK(cudaMemcpyAsync(arr64(d, b, q), src[q], n * sizeof(double),
+                                          cudaMemcpyDeviceToDevice, d->streams[stream]));
+        else
+            AC_CUDA_CHECK(ac_launch_split(d->geom, src[q], arr_hi(d, b, q), arr_lo(d, b, q),
+                                          d->streams[stream], &d->launches));
+    }
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceStoreMeshDevice(const Device d, const Stream stream, AcReal* const* dst)
+{
+    if (!d || !dst || !stream_ok(stream))
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    const size_t n = (size_t)d->geom.mx * d->geom.my * d->geom.mz;
+    for (int q = 0; q < AC_NF; ++q) {
+        if (!dst[q])
+            return AC_NOT_ALLOCATED;
+        const int b = d->in_idx[q];
+        if (d->precision == 0)
+            AC_CUDA_CHECK(cudaMemcpyAsync(dst[q], arr64(d, b, q), n * sizeof(double),
+                                          cudaMemcpyDeviceToDevice, d->streams[stream]));
+        else
+            AC_CUDA_CHECK(ac_launch_join(d->geom, arr_hi(d, b, q), arr_lo(d, b, q), dst[q],
+                                         d->streams[stream], &d->launches));
+    }
+    return AC_SUCCESS;
+}
+
+/* ---- discrete adjoint ---- */
+
+static AcResult
+ensure_adjoint(const Device d)
+{
+    if (d->precision != 0) {
+        fprintf(stderr, "astaroth_b200: the adjoint needs an FP64 device (AC_precision = 0)\n");
+        return AC_FAILURE;
+    }
+    if (d->adj_lf)
+        return AC_SUCCESS;
+    const size_t fb = (size_t)d->geom.cells * sizeof(double);
+    AC_CUDA_CHECK(cudaMalloc((void**)&d->adj_lf, AC_NF * fb));
+    AC_CUDA_CHECK(cudaMalloc((void**)&d->adj_lw, AC_NF * fb));
+    AC_CUDA_CHECK(cudaMalloc((void**)&d->adj_mu, AC_MU_COUNT * fb));
+    AC_CUDA_CHECK(cudaMalloc((void**)&d->adj_pgrad, 2 * sizeof(double)));
+    AC_CUDA_CHECK(cudaMemset(d->adj_mu, 0, AC_MU_COUNT * fb));
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceLoadAdjoint(const Device d, const Stream stream, const AcReal* const* lam_f)
+{
+    if (!d || !stream_ok(stream))
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    if (ensure_adjoint(d) != AC_SUCCESS)
+        return AC_FAILURE;
+    cudaStream_t st = d->streams[stream];
+    const size_t fb = (size_t)d->geom.cells * sizeof(double);
+    for (int q = 0; q < AC_NF; ++q) {
+        if (lam_f && lam_f[q])
+            AC_CUDA_CHECK(cudaMemcpyAsync(d->adj_lf + (size_t)q * d->geom.cells, lam_f[q], fb,
+                                          cudaMemcpyDeviceToDevice, st));
+        else
+            AC_CUDA_CHECK(cudaMemsetAsync(d->adj_lf + (size_t)q * d->geom.cells, 0, fb, st));
+    }
+    AC_CUDA_CHECK(cudaMemsetAsync(d->adj_lw, 0, AC_NF * fb, st));
+    AC_CUDA_CHECK(cudaMemsetAsync(d->adj_pgrad, 0, 2 * sizeof(double), st));
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceStoreAdjoint(const Device d, const Stream stream, AcReal* const* lam_f)
+{
+    if (!d || !lam_f || !stream_ok(stream) || !d->adj_lf)
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    const size_t fb = (size_t)d->geom.cells * sizeof(double);
+    for (int q = 0; q < AC_NF; ++q)
+        if (lam_f[q])
+            AC_CUDA_CHECK(cudaMemcpyAsync(lam_f[q], d->adj_lf + (size_t)q * d->geom.cells, fb,
+                                          cudaMemcpyDeviceToDevice, d->streams[stream]));
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceIntegrateSubstepAdjoint(const Device d, const Stream stream, const int step_number,
+                                const Volume start, const Volume end, const AcReal dt)
+{
+    if (!d || !stream_ok(stream) || step_number < 0 || step_number > 2 || !d->adj_lf)
+        return AC_FAILURE;
+    if (!is_whole_interior(d, start, end)) {
+        fprintf(stderr, "astaroth_b200: acDeviceIntegrateSubstepAdjoint needs the whole interior\n");
+        return AC_FAILURE;
+    }
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    StencilCoef sc;
+    PhysConst pc;
+    ac_make_stencil(d->config, &sc);
+    ac_make_phys(d->config, &pc);
+    AdjointFields a;
+    for (int q = 0; q < AC_NF; ++q) {
+        a.f[q]  = arr64(d, d->in_idx[q], q);
+        a.lf[q] = d->adj_lf + (size_t)q * d->geom.cells;
+        a.lw[q] = d->adj_lw + (size_t)q * d->geom.cells;
+    }
+    for (int m = 0; m < AC_MU_COUNT; ++m)
+        a.mu[m] = d->adj_mu + (size_t)m * d->geom.cells;
+    const double alpha[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
+    const double beta[3]  = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
+    AC_CUDA_CHECK(ac_launch_adjoint_substep(d->geom, a, sc, pc, alpha[step_number],
+                                            beta[step_number], dt, d->adj_pgrad,
+                                            d->streams[stream], &d->launches));
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceGetParamAdjoints(const Device d, AcReal* nu_bar, AcReal* eta_bar)
+{
+    if (!d || !nu_bar || !eta_bar || !d->adj_pgrad)
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    for (int s = 0; s < NUM_STREAMS; ++s)
+        AC_CUDA_CHECK(cudaStreamSynchronize(d->streams[s]));
+    double v[2];
+    AC_CUDA_CHECK(cudaMemcpy(v, d->adj_pgrad, sizeof(v), cudaMemcpyDeviceToHost));
+    *nu_bar  = v[0];
+    *eta_bar = v[1];
     return AC_SUCCESS;
 }
 

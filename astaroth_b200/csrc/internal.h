@@ -115,6 +115,16 @@ struct ReduceScratch {
     int max_blocks;
 };
 
+/* Adjoint state of one device (FP64 only): adjoints of f and w per field, the
+ * 46 derivative-slot adjoints mu, and the parameter adjoints (nu, eta). */
+#define AC_MU_COUNT 46
+struct AdjointFields {
+    const double* f[AC_NF];
+    double* lf[AC_NF];
+    double* lw[AC_NF];
+    double* mu[AC_MU_COUNT];
+};
+
 struct StepGraph {
     cudaGraphExec_t exec;
     double dt;
@@ -144,6 +154,11 @@ struct device_s {
     double* host_result; /* pinned */
     StepGraph graphs[NUM_STREAMS][2];
     int solve_variant;   /* 0 = plain, 1 = tiled */
+    /* adjoint buffers, allocated by the first acDeviceLoadAdjoint */
+    double* adj_lf;      /* 8 fields */
+    double* adj_lw;      /* 8 fields */
+    double* adj_mu;      /* AC_MU_COUNT fields */
+    double* adj_pgrad;   /* 2 values: d/d nu, d/d eta */
     unsigned long long launches;
 };
 
@@ -201,6 +216,13 @@ template <typename T>
 cudaError_t ac_launch_cfl(const Geom& g, const FieldsT<T>& f, const StencilCoef& sc,
                           const double cs2_sound, unsigned long long* cfl, cudaStream_t stream,
                           unsigned long long* launches);
+
+/* One adjoint substep (adjoint.cu): local reverse + halo fill of mu + gather. */
+cudaError_t ac_launch_adjoint_substep(const Geom& g, const AdjointFields& a,
+                                      const StencilCoef& sc, const PhysConst& pc,
+                                      const double alpha, const double beta, const double dt,
+                                      double* pgrad, cudaStream_t stream,
+                                      unsigned long long* launches);
 
 /* Host-side setup helpers (device.cu). */
 void ac_make_stencil(const AcMeshInfo& info, StencilCoef* sc);

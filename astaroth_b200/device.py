@@ -241,6 +241,43 @@ class Device:
         _check(self.lib.acDeviceGetTimestep(self._h, C.byref(dt)), "acDeviceGetTimestep")
         return dt.value
 
+    # ---- caller-owned device arrays (torch tensors of shape (8, mz, my, mx), float64) ----
+    @staticmethod
+    def _ptrs(t):
+        if t is None:
+            return None
+        if t.dtype.__str__() != "torch.float64" or not t.is_contiguous() or t.shape[0] != 8:
+            raise ValueError("expected a contiguous float64 tensor of shape (8, mz, my, mx)")
+        return (C.c_void_p * 8)(*[t[q].data_ptr() for q in range(8)])
+
+    def load_mesh_device(self, t, stream: int = 0) -> None:
+        _check(self.lib.acDeviceLoadMeshDevice(self._h, stream, self._ptrs(t)),
+               "acDeviceLoadMeshDevice")
+
+    def store_mesh_device(self, t, stream: int = 0):
+        _check(self.lib.acDeviceStoreMeshDevice(self._h, stream, self._ptrs(t)),
+               "acDeviceStoreMeshDevice")
+        return t
+
+    def load_adjoint(self, t=None, stream: int = 0) -> None:
+        _check(self.lib.acDeviceLoadAdjoint(self._h, stream, self._ptrs(t)), "acDeviceLoadAdjoint")
+
+    def store_adjoint(self, t, stream: int = 0):
+        _check(self.lib.acDeviceStoreAdjoint(self._h, stream, self._ptrs(t)),
+               "acDeviceStoreAdjoint")
+        return t
+
+    def integrate_substep_adjoint(self, step: int, dt: float, stream: int = 0) -> None:
+        _check(self.lib.acDeviceIntegrateSubstepAdjoint(self._h, stream, step, self.vols.n0,
+                                                        self.vols.n1, dt),
+               "acDeviceIntegrateSubstepAdjoint")
+
+    def param_adjoints(self):
+        nu, eta = C.c_double(), C.c_double()
+        _check(self.lib.acDeviceGetParamAdjoints(self._h, C.byref(nu), C.byref(eta)),
+               "acDeviceGetParamAdjoints")
+        return nu.value, eta.value
+
     # ---- introspection ----
     def stream_handle(self, stream: int = 0) -> int:
         return self.lib.acDeviceGetStreamHandle(self._h, stream) or 0

@@ -149,3 +149,26 @@ def test_rates_match_numpy_stencils():
            u[0] * B[1] - u[1] * B[0] + p["eta"] * lap(a[2])]
     for got, want in [(r[0], cont)] + [(r[4 + c], ind[c]) for c in range(3)]:
         assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+
+
+def test_torch_reference_matches_oracle():
+    """The torch restatement used for CPU reference gradients agrees with the oracle."""
+    import sys
+    import torch
+    sys.path.insert(0, str(Path(__file__).resolve().parent))
+    import mhd_torch_ref as R
+    info = make_info((12, 10, 8), **CONFIG_PARAMS)
+    p = info_to_dict(info)
+    f = seeded_mesh(info, 5, amp_scalar=0.1, sigma_uu=0.05, sigma_aa=0.02)
+    oracle.periodic_bounds(f, "port")
+    r_or = oracle.interior(oracle.rates(f, p))
+    r_t = R.rates(torch.from_numpy(oracle.interior(f).copy()), p).numpy()
+    err = np.abs(r_t - r_or).reshape(8, -1).max(1) / np.abs(r_or).reshape(8, -1).max(1)
+    assert err.max() <= 1e-14
+    a = f.copy()
+    oracle.integrate(a, p, 2e-3, 3, "port")
+    x = torch.from_numpy(oracle.interior(f).copy())
+    for _ in range(3):
+        x = R.step(x, p, 2e-3)
+    err = oracle.rel_linf(np.pad(x.numpy(), ((0, 0),) + ((3, 3),) * 3), a)
+    assert err.max() <= 1e-14
