@@ -250,21 +250,36 @@ class Device:
             raise ValueError("expected a contiguous float64 tensor of shape (8, mz, my, mx)")
         return (C.c_void_p * 8)(*[t[q].data_ptr() for q in range(8)])
 
+    # The library works on its own non-blocking streams, which do not order
+    # against torch's stream: a read of a torch tensor first waits for torch's
+    # pending work, and a write into one completes before the call returns.
+    @staticmethod
+    def _torch_ready(t) -> None:
+        if t is not None:
+            import torch
+            torch.cuda.current_stream(t.device).synchronize()
+
     def load_mesh_device(self, t, stream: int = 0) -> None:
+        self._torch_ready(t)
         _check(self.lib.acDeviceLoadMeshDevice(self._h, stream, self._ptrs(t)),
                "acDeviceLoadMeshDevice")
 
     def store_mesh_device(self, t, stream: int = 0):
+        self._torch_ready(t)
         _check(self.lib.acDeviceStoreMeshDevice(self._h, stream, self._ptrs(t)),
                "acDeviceStoreMeshDevice")
+        self.synchronize(stream)
         return t
 
     def load_adjoint(self, t=None, stream: int = 0) -> None:
+        self._torch_ready(t)
         _check(self.lib.acDeviceLoadAdjoint(self._h, stream, self._ptrs(t)), "acDeviceLoadAdjoint")
 
     def store_adjoint(self, t, stream: int = 0):
+        self._torch_ready(t)
         _check(self.lib.acDeviceStoreAdjoint(self._h, stream, self._ptrs(t)),
                "acDeviceStoreAdjoint")
+        self.synchronize(stream)
         return t
 
     def integrate_substep_adjoint(self, step: int, dt: float, stream: int = 0) -> None:
