@@ -3,11 +3,11 @@ function of the initial fields and of nu, eta.
 
 Forward: N RK3 steps of the device integrator (acDeviceIntegrateStep), with a
 checkpoint of the state every k steps.  Backward: for each checkpoint segment,
-from the last to the first, the states at the start of its steps are
-recomputed, and for each step (last first) the substep states f_0, f_1, f_2
-are recomputed and the discrete adjoint substeps s = 2, 1, 0 are applied
-(acDeviceIntegrateSubstepAdjoint).  Memory: the checkpoints, one segment of
-step states and three substep states, so O(N/k + k) meshes instead of O(N).
+from the last to the first, the segment is integrated again from its
+checkpoint, keeping the three substep states f_0, f_1, f_2 of every step; then
+for each step (last first) the discrete adjoint substeps s = 2, 1, 0 are
+applied (acDeviceIntegrateSubstepAdjoint).  Every step is recomputed once.
+Memory: N/k checkpoints plus 3k substep states.
 
 Tensors are (8, mz, my, mx) float64 on the GPU (halos included, as the host
 AcMesh).  The integration fills the halos itself, so gradients live on the
@@ -80,33 +80,29 @@ class _Integrate(torch.autograd.Function):
         dev.set_real(capi.RealParam.AC_eta, ctx.eta)
         lam = torch.zeros_like(grad_out)
         interior(lam).copy_(interior(grad_out))
-        dev.load_adjoint(lam.contiguous())
-        nseg = len(ctx.ckpts)
-        for seg in reversed(range(nseg)):
+        dev.load_adjoint(lam)
+        # substep states f_0, f_1, f_2 of every step of one segment; written and
+        # read only by the device's stream, so no per-transfer synchronisation
+        buf = [torch.empty_like(grad_out) for _ in range(3 * min(every, steps))]
+        torch.cuda.synchronize()
+        for seg in reversed(range(len(ctx.ckpts))):
             n0 = seg * every
             n1 = min(n0 + every, steps)
-            # states at the start of the segment's steps
-            states = [ctx.ckpts[seg]]
-            dev.load_mesh_device(ctx.ckpts[seg])
-            for _ in range(n0, n1 - 1):
-                dev.integrate_step(dt)
-                states.append(dev.store_mesh_device(torch.empty_like(grad_out)))
-            for n in reversed(range(n1 - n0)):
-                # substep states f_0, f_1, f_2 of this step
-                sub = [states[n]]
-                dev.load_mesh_device(states[n])
-                for s in (0, 1):
+            dev.load_mesh_device(ctx.ckpts[seg], wait_torch=False)
+            for n in range(n1 - n0):
+                for s in range(3):
+                    dev.store_mesh_device(buf[3 * n + s], sync=False)
+                    if n == n1 - n0 - 1 and s == 2:
+                        break  # the segment's final state is not needed
                     dev.periodic_boundconds()
                     dev.integrate_substep(s, dt)
                     dev.swap_buffers()
-                    sub.append(dev.store_mesh_device(torch.empty_like(grad_out)))
+            for n in reversed(range(n1 - n0)):
                 for s in (2, 1, 0):
-                    dev.load_mesh_device(sub[s])
+                    dev.load_mesh_device(buf[3 * n + s], wait_torch=False)
                     dev.periodic_boundconds()
                     dev.integrate_substep_adjoint(s, dt)
-        g0 = torch.zeros_like(grad_out)
-        dev.store_adjoint(g0)
-        torch.cuda.synchronize()
+        g0 = dev.store_adjoint(torch.zeros_like(grad_out))
         out = torch.zeros_like(g0)
         interior(out).copy_(interior(g0))
         nu_bar, eta_bar = dev.param_adjoints()

@@ -259,16 +259,21 @@ class Device:
             import torch
             torch.cuda.current_stream(t.device).synchronize()
 
-    def load_mesh_device(self, t, stream: int = 0) -> None:
-        self._torch_ready(t)
+    def load_mesh_device(self, t, stream: int = 0, wait_torch: bool = True) -> None:
+        """wait_torch=False when t was last written by this device's own stream."""
+        if wait_torch:
+            self._torch_ready(t)
         _check(self.lib.acDeviceLoadMeshDevice(self._h, stream, self._ptrs(t)),
                "acDeviceLoadMeshDevice")
 
-    def store_mesh_device(self, t, stream: int = 0):
-        self._torch_ready(t)
+    def store_mesh_device(self, t, stream: int = 0, sync: bool = True):
+        """sync=False when only this device's stream reads t afterwards."""
+        if sync:
+            self._torch_ready(t)
         _check(self.lib.acDeviceStoreMeshDevice(self._h, stream, self._ptrs(t)),
                "acDeviceStoreMeshDevice")
-        self.synchronize(stream)
+        if sync:
+            self.synchronize(stream)
         return t
 
     def load_adjoint(self, t=None, stream: int = 0) -> None:
