@@ -169,6 +169,11 @@ RTYPES = {
 RTYPE_INDEX = {name: i for i, name in enumerate(RTYPES)}
 
 Device_p = C.c_void_p
+Ensemble_p = C.c_void_p
+
+
+class AcEnsembleTiles(C.Structure):
+    _fields_ = [("tx", C.c_int), ("ty", C.c_int), ("zb", C.c_int), ("blocks_per_sm", C.c_int)]
 
 # name -> (restype, argtypes)
 SIGNATURES = {
@@ -241,6 +246,26 @@ SIGNATURES = {
     "acB200Version": (C.c_char_p, []),
     "acReduceNoAlloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int, C.c_int,
                                   AcReduction, C.c_void_p, C.c_int, C.c_void_p]),
+    "acEnsembleCreate": (C.c_int, [C.c_int, C.c_int, C.POINTER(AcMeshInfo),
+                                   C.POINTER(Ensemble_p)]),
+    "acEnsembleDestroy": (C.c_int, [C.POINTER(Ensemble_p)]),
+    "acEnsembleLoadMember": (C.c_int, [Ensemble_p, C.c_int, AcMesh]),
+    "acEnsembleStoreMember": (C.c_int, [Ensemble_p, C.c_int, C.POINTER(AcMesh)]),
+    "acEnsembleSetTimesteps": (C.c_int, [Ensemble_p, C.POINTER(C.c_double)]),
+    "acEnsembleIntegrateStep": (C.c_int, [Ensemble_p]),
+    "acEnsembleIntegrateStepSequential": (C.c_int, [Ensemble_p]),
+    "acEnsembleSetTiles": (C.c_int, [Ensemble_p, AcEnsembleTiles]),
+    "acEnsembleGetTiles": (C.c_int, [Ensemble_p, C.POINTER(AcEnsembleTiles)]),
+    "acEnsembleAutotune": (C.c_int, [Ensemble_p, C.POINTER(AcEnsembleTiles),
+                                     C.POINTER(C.c_double)]),
+    "acEnsembleReduceScal": (C.c_int, [Ensemble_p, C.c_int, AcReduction, C.c_int,
+                                       C.POINTER(C.c_double)]),
+    "acEnsembleReduceVec": (C.c_int, [Ensemble_p, C.c_int, AcReduction, C.c_int, C.c_int,
+                                      C.c_int, C.POINTER(C.c_double)]),
+    "acEnsembleSynchronize": (C.c_int, [Ensemble_p]),
+    "acEnsembleGetStreamHandle": (C.c_void_p, [Ensemble_p]),
+    "acEnsembleGetLaunchCount": (C.c_ulonglong, [Ensemble_p]),
+    "acEnsembleCellCount": (C.c_longlong, [Ensemble_p]),
 }
 
 # acReduceNoAlloc accepts at most this many thread blocks (its static scratch).

@@ -17,6 +17,7 @@
  * no thread is spent on the interior.
  */
 #include "internal.h"
+#include "halo.cuh"
 
 namespace {
 
@@ -34,11 +35,8 @@ template <typename T>
 __device__ __forceinline__ void
 copy_wrapped(const Geom& g, const ArrayList<T>& fl, const int i, const int j, const int k)
 {
-    const int is = (i - NGHOST + g.nx) % g.nx + NGHOST;
-    const int js = (j - NGHOST + g.ny) % g.ny + NGHOST;
-    const int ks = (k - NGHOST + g.nz) % g.nz + NGHOST;
     const long long dst = geom_idx(g, i, j, k);
-    const long long src = geom_idx(g, is, js, ks);
+    const long long src = halo_source(g, i, j, k);
 #pragma unroll
     for (int q = 0; q < kMaxArrays; ++q)
         if (q < fl.n)
@@ -54,28 +52,8 @@ periodic_halo_kernel(const Geom g, const ArrayList<T> fl, const long long nzs,
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= total)
         return;
-    const long long mxy = (long long)g.mx * g.my;
     int i, j, k;
-    if (t < nzs) { /* z slabs: 2*NGHOST full planes */
-        i            = (int)(t % g.mx);
-        j            = (int)((t / g.mx) % g.my);
-        const int kk = (int)(t / mxy);
-        k            = kk < NGHOST ? kk : g.nz + kk;
-    }
-    else if (t < nzs + nys) { /* y slabs inside the interior z range */
-        const long long u = t - nzs;
-        i                 = (int)(u % g.mx);
-        const int jj      = (int)((u / g.mx) % (2 * NGHOST));
-        k                 = NGHOST + (int)(u / ((long long)g.mx * 2 * NGHOST));
-        j                 = jj < NGHOST ? jj : g.ny + jj;
-    }
-    else { /* x slabs inside the interior y and z ranges */
-        const long long u = t - nzs - nys;
-        const int ii      = (int)(u % (2 * NGHOST));
-        j                 = NGHOST + (int)((u / (2 * NGHOST)) % g.ny);
-        k                 = NGHOST + (int)(u / ((long long)2 * NGHOST * g.ny));
-        i                 = ii < NGHOST ? ii : g.nx + ii;
-    }
+    halo_cell(g, t, nzs, nys, i, j, k);
     copy_wrapped(g, fl, i, j, k);
 }
 
@@ -175,10 +153,8 @@ ac_launch_periodic(const Geom& g, T* const* arrays, const int n, const Volume st
     const bool whole = start.x == 0 && start.y == 0 && start.z == 0 && end.x == (size_t)g.mx &&
                        end.y == (size_t)g.my && end.z == (size_t)g.mz;
     if (whole) {
-        const long long nzs   = 2LL * NGHOST * g.mx * g.my;
-        const long long nys   = 2LL * NGHOST * g.mx * g.nz;
-        const long long nxs   = 2LL * NGHOST * g.ny * g.nz;
-        const long long total = nzs + nys + nxs;
+        long long nzs, nys;
+        const long long total = halo_count(g, &nzs, &nys);
         const int tpb         = 256;
         const long long bpg   = (total + tpb - 1) / tpb;
         periodic_halo_kernel<T><<<(unsigned)bpg, tpb, 0, stream>>>(g, fl, nzs, nys, total);

@@ -607,8 +607,8 @@ is_whole_interior(const Device d, const Volume start, const Volume end)
            end.z == (size_t)(d->geom.nz + NGHOST);
 }
 
-static RkCoef
-rk_coef(const int step, const double dt)
+RkCoef
+ac_rk_coef(const int step, const double dt)
 {
     /* Williamson 2N RK3, acc-runtime/stdlib/integrators.h:11-13 */
     const double alpha[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
@@ -629,7 +629,7 @@ launch_substep(Device d, cudaStream_t st, const int step, const double dt,
     PhysConst pc;
     ac_make_stencil(d->config, &sc);
     ac_make_phys(d->config, &pc);
-    const RkCoef rk = rk_coef(step, dt);
+    const RkCoef rk = ac_rk_coef(step, dt);
     const int blk   = in_block_index(d);
     const bool tiled = d->solve_variant == 1 && d->tmap_ok && blk >= 0;
     /* substep 2 also produces the CFL maxima of its input state, as the

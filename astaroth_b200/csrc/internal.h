@@ -228,3 +228,5 @@ cudaError_t ac_launch_adjoint_substep(const Geom& g, const AdjointFields& a,
 void ac_make_stencil(const AcMeshInfo& info, StencilCoef* sc);
 void ac_make_phys(const AcMeshInfo& info, PhysConst* pc);
 Geom ac_make_geom(const AcMeshInfo& info, const int precision);
+/* Coefficients of RK3 substep `step` (0, 1, 2) with timestep dt. */
+RkCoef ac_rk_coef(const int step, const double dt);

@@ -170,3 +170,25 @@ def test_device_create_fails_cleanly_without_gpu():
     assert not h
     with pytest.raises(ab.AstarothError):
         ab.Device(info)
+
+
+def test_ensemble_members_seeded():
+    from astaroth_b200.ensemble import ENSEMBLE_SIZES, ensemble_members
+
+    a = ensemble_members(64)
+    b = ensemble_members(64)
+    assert [capi_dims(i) for i, _ in a] == [capi_dims(i) for i, _ in b]
+    assert [s for _, s in a] == list(range(100, 164))
+    sizes = {capi_dims(i)[0] for i, _ in a}
+    assert sizes <= set(ENSEMBLE_SIZES) and len(sizes) == len(ENSEMBLE_SIZES)
+    for info, _ in a:
+        nu = info.real_params[capi.RealParam.AC_nu_visc]
+        eta = info.real_params[capi.RealParam.AC_eta]
+        assert 1e-3 <= nu <= 1e-2 and 1e-3 <= eta <= 1e-2
+        assert info.int_params[capi.IntParam.AC_precision] == 1
+
+
+def capi_dims(info):
+    from astaroth_b200.device import dims
+
+    return dims(info)

@@ -1,0 +1,179 @@
+"""Ensemble (acEnsemble*) parity on the GPU.
+
+Every member of an ensemble must equal, bit for bit, a single-mesh Device of
+the same config without tiling (AC_debug_plain_kernel = 1) after the same
+steps: the persistent launch computes each cell with the plain kernel's
+per-cell function.  The graph step, the sequential per-member launches and any
+tile shape give the same bits.  FP64 members are also checked against the
+oracle after one step.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from astaroth_b200 import capi
+from astaroth_b200.device import AstarothError, Device, make_info, seeded_mesh
+from astaroth_b200.ensemble import Ensemble, ensemble_members
+
+pytestmark = pytest.mark.gpu
+
+DT = 1e-3
+
+
+def _members(precision, shapes, seed0=100):
+    rng = np.random.default_rng(7)
+    infos = []
+    for n in shapes:
+        nu, eta = 10.0 ** rng.uniform(-3, -2, size=2)
+        infos.append(make_info(n, precision=precision, nu_visc=nu, eta=eta))
+    return infos, [seed0 + m for m in range(len(infos))]
+
+
+def _device_run(info, seed, steps, dt=DT):
+    info.int_params[capi.IntParam.AC_debug_plain_kernel] = 1
+    with Device(info) as d:
+        f = seeded_mesh(info, seed)
+        d.load_mesh(f)
+        for _ in range(steps):
+            d.integrate_step(dt)
+        d.synchronize()
+        out = d.store_mesh()
+    info.int_params[capi.IntParam.AC_debug_plain_kernel] = 0
+    return out
+
+
+SHAPES = [32, 48, (40, 36, 44), 64, 33, 96]
+
+
+@pytest.mark.parametrize("precision", [1, 0])
+def test_members_equal_single_device(precision):
+    infos, seeds = _members(precision, SHAPES)
+    steps = 3
+    with Ensemble(infos) as e:
+        e.load_seeded(seeds)
+        e.set_timesteps(DT)
+        for _ in range(steps):
+            e.integrate_step()
+        e.synchronize()
+        got = [e.store_member(m) for m in range(e.n)]
+    for m, (info, seed) in enumerate(zip(infos, seeds)):
+        ref = _device_run(info, seed, steps)
+        assert np.array_equal(got[m], ref), f"member {m} differs from its single-mesh run"
+
+
+def test_graph_sequential_and_tiles_agree():
+    infos, seeds = _members(1, SHAPES)
+    outs = []
+    for mode in ("graph", "sequential", "tiles"):
+        with Ensemble(infos) as e:
+            e.load_seeded(seeds)
+            e.set_timesteps(DT)
+            if mode == "tiles":
+                e.set_tiles(16, 8, 5, 1)
+                assert e.tiles == (16, 8, 5, 1)
+            for _ in range(2):
+                if mode == "sequential":
+                    e.integrate_step_sequential()
+                else:
+                    e.integrate_step()
+            e.synchronize()
+            outs.append([e.store_member(m) for m in range(e.n)])
+    for m in range(len(infos)):
+        assert np.array_equal(outs[0][m], outs[1][m])
+        assert np.array_equal(outs[0][m], outs[2][m])
+
+
+def test_autotune_keeps_state_and_results(tmp_path):
+    infos, seeds = _members(1, [32, 48, 64])
+    with Ensemble(infos) as e:
+        e.load_seeded(seeds)
+        e.set_timesteps(DT)
+        before = [e.store_member(m) for m in range(e.n)]
+        tiles, ms = e.autotune(cache=tmp_path / "tiles.json")
+        assert ms is not None and ms > 0
+        tx, ty, zb, bps = tiles
+        assert tx * ty % 32 == 0 and tx * ty <= 256 and zb >= 1
+        for m in range(e.n):  # tuning leaves the in-buffers as they were
+            assert np.array_equal(e.store_member(m), before[m])
+        e.integrate_step()
+        e.synchronize()
+        got = [e.store_member(m) for m in range(e.n)]
+        # a second ensemble takes the tiles from the cache
+        with Ensemble(infos) as e2:
+            t2, ms2 = e2.autotune(cache=tmp_path / "tiles.json")
+            assert t2 == tiles and ms2 is None
+    for m in range(len(infos)):
+        assert np.array_equal(got[m], _device_run(infos[m], seeds[m], 1))
+
+
+def test_fp64_member_matches_oracle():
+    infos, seeds = _members(0, [32, (24, 40, 32)])
+    with Ensemble(infos) as e:
+        e.load_seeded(seeds)
+        e.set_timesteps(DT)
+        e.integrate_step()
+        e.synchronize()
+        for m in range(e.n):
+            from astaroth_b200.device import info_to_dict
+            f0 = seeded_mesh(infos[m], seeds[m])
+            ref = oracle.integrate(f0, info_to_dict(infos[m]), DT, 1)
+            got = e.store_member(m)
+            for q in range(8):
+                assert oracle.rel_linf(oracle.interior(got[q]), oracle.interior(ref[q])) <= 1e-12
+
+
+def test_member_reductions_match_device():
+    infos, seeds = _members(1, [32, 48])
+    with Ensemble(infos) as e:
+        e.load_seeded(seeds)
+        for m in range(e.n):
+            with Device(infos[m]) as d:
+                d.load_mesh(seeded_mesh(infos[m], seeds[m]))
+                for rt in ("RTYPE_MAX", "RTYPE_MIN", "RTYPE_RMS", "RTYPE_RMS_EXP"):
+                    assert e.reduce_scal(m, rt, 0) == d.reduce_scal(rt, 0)
+                assert e.reduce_vec(m, "RTYPE_RMS", 1, 2, 3) == d.reduce_vec("RTYPE_RMS", 1, 2, 3)
+
+
+def test_errors():
+    infos, seeds = _members(1, [32, 32])
+    with Ensemble(infos) as e:
+        with pytest.raises(AstarothError):
+            e.store_member(5)
+        with pytest.raises(AstarothError):
+            e.set_tiles(7, 3, 4)  # 21 threads: not a multiple of 32
+        with pytest.raises(AstarothError):
+            e.load_member(0, seeded_mesh(make_info(48, precision=1), 1))  # wrong size
+        with pytest.raises(AstarothError):
+            e.reduce_scal(0, "RTYPE_ALFVEN_MAX", 0)
+    with pytest.raises(AstarothError):
+        Ensemble([make_info(32, precision=0), make_info(32, precision=1)])
+
+
+def test_config3_ensemble_graph_equals_sequential():
+    """The 64-member FP32-compensated ensemble: graph == sequential launches
+    after 2 steps; prints both rates."""
+    import time
+
+    members = ensemble_members(64)
+    infos = [i for i, _ in members]
+    seeds = [s for _, s in members]
+    outs, rates = [], {}
+    for mode in ("graph", "sequential"):
+        with Ensemble(infos) as e:
+            e.load_seeded(seeds)
+            e.set_timesteps(DT)
+            if mode == "graph":
+                e.autotune(use_cache=False)
+            for _ in range(2):
+                e.integrate_step() if mode == "graph" else e.integrate_step_sequential()
+            e.synchronize()
+            outs.append([e.store_member(m) for m in (0, 17, 63)])
+            t0 = time.perf_counter()
+            for _ in range(5):
+                e.integrate_step() if mode == "graph" else e.integrate_step_sequential()
+            e.synchronize()
+            rates[mode] = 5 * e.cells / (time.perf_counter() - t0)
+    print(f"config3: {rates['graph']:.3e} cell-updates/s (graph, persistent), "
+          f"{rates['sequential']:.3e} (sequential plain launches)")
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
