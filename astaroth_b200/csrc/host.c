@@ -294,7 +294,7 @@ acHostMeshRandomizeSeeded(AcMesh* mesh, const unsigned long long seed, const AcR
     for (int w = 0; w < NUM_VTXBUF_HANDLES; ++w) {
         AcReal* f = mesh->vertex_buffer[w];
         if (!f)
-            return AC_FAILURE;
+            continue; /* fields without a buffer are skipped */
         const int gaussian = (w >= VTXBUF_UUX && w <= VTXBUF_AZ);
         const double sigma = (w <= VTXBUF_UUZ) ? sigma_uu : sigma_aa;
         const uint64_t fbase = base + (uint64_t)w * 0x9E3779B97F4A7C15ull * 2ull * (uint64_t)n;
@@ -418,6 +418,14 @@ acHostMeshSolenoidalModes(AcMesh* mesh, const unsigned long long seed, const int
     AcReal* ux = mesh->vertex_buffer[VTXBUF_UUX];
     AcReal* uy = mesh->vertex_buffer[VTXBUF_UUY];
     AcReal* uz = mesh->vertex_buffer[VTXBUF_UUZ];
+    if (!ux || !uy || !uz) {
+        for (int a = 0; a < 3; ++a)
+            free(tab[a]);
+        free(kv);
+        free(av);
+        free(ph);
+        return AC_FAILURE;
+    }
 #pragma omp parallel for schedule(static)
     for (int k = 0; k < m.z; ++k) {
         double* cyz = (double*)malloc(sizeof(double) * 2 * (size_t)nmodes);

@@ -83,11 +83,18 @@ class Ensemble:
             pass
 
     # ---- data ----
+    def _member(self, m: int) -> int:
+        if not 0 <= m < self.n:
+            raise AstarothError(f"ensemble member {m} out of range [0, {self.n})")
+        return m
+
     def load_member(self, m: int, fields: np.ndarray) -> None:
+        self._member(m)
         _check(self.lib.acEnsembleLoadMember(self._h, m, mesh_struct(fields, self.infos[m])),
                "acEnsembleLoadMember")
 
     def store_member(self, m: int, out: np.ndarray | None = None) -> np.ndarray:
+        self._member(m)
         out = empty_mesh(self.infos[m]) if out is None else out
         mesh = mesh_struct(out, self.infos[m])
         _check(self.lib.acEnsembleStoreMember(self._h, m, C.byref(mesh)), "acEnsembleStoreMember")

@@ -19,6 +19,9 @@ aa ~ N(0, 1e-4^2)), nu = eta = 5e-3, cs = 1, gamma = 5/3, dt = 1e-3.
               against the measured HBM copy bandwidth.
 * cpu_baseline  the reference's own host model (oracle/_ref) on the host cores,
               a bounded sample (one RK3 step at 96^3), rank 0 at N=1.
+* ensemble    64 independent FP32-compensated members of sizes {32,48,64,96}^3
+              in one persistent launch per substep, graph-captured step, tiles
+              from the autotuner; against sequential per-member plain launches.
 * fp32comp    the same workload with FP32 fields and a compensated FP32 hi/lo RK3
               state (AC_precision = 1): cell-updates/s, speed-up over FP64, and
               the per-field relative L-inf against the FP64 path after 100 steps
@@ -61,6 +64,10 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32comp", action="store_true")
+    ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--workload", default="step512", choices=["step512", "cfl1024"],
+                    help="step512: the FP64 RK3 step (default line); cfl1024: 1024^3 "
+                         "FP32-compensated run with adaptive CFL timesteps")
     ap.add_argument("--accuracy-steps", type=int, default=100)
     return ap.parse_args()
 
@@ -307,6 +314,10 @@ def run_gpu(args):
     if world == 1 and not args.no_fp32comp:
         fp32 = fp32comp_leg(args, ab, torch, host, dev, info)
 
+    ens = None
+    if not args.no_ensemble:
+        ens = ensemble_leg(args, torch, rank, world)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -333,7 +344,7 @@ def run_gpu(args):
                          "peak_source": peak_kind, "solve_ms_per_step": solve_step_ms,
                          "boundconds_ms_per_step": sum(bc_ms[-3:])},
             "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
-            "fp32comp": fp32,
+            "fp32comp": fp32, "ensemble": ens,
         }
         if fp32 and "ms_per_step" in fp32:
             fp32["speedup_vs_fp64"] = t_max / fp32["ms_per_step"]
@@ -418,8 +429,195 @@ def fp32comp_leg(args, ab, torch, host, dev64, info64):
     return out
 
 
+def ensemble_leg(args, torch, rank, world):
+    """The 64-member FP32-compensated ensemble (N in {32, 48, 64, 96}, nu and
+    eta log-uniform on [1e-3, 1e-2], seeds 100..163, dt = 1e-3): members are
+    sharded across ranks (no data-path collective); each rank advances its
+    members with the graph-captured persistent step and, for comparison, with
+    sequential per-member plain launches."""
+    from astaroth_b200 import dist as adist
+    from astaroth_b200.ensemble import Ensemble, ensemble_members
+
+    members = ensemble_members(64)
+    costs = [abs(ab_cells(i)) for i, _ in members]
+    mine = adist.shard(costs, rank, world)
+    total_cells = sum(costs)
+    e = Ensemble([members[m][0] for m in mine], device_id=torch.cuda.current_device())
+    e.load_seeded([members[m][1] for m in mine])
+    e.set_timesteps(1e-3)
+    tiles, tune_ms = e.autotune(use_cache=False)
+    stream = torch.cuda.ExternalStream(e.stream_handle())
+
+    def timed(step, k):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        adist.barrier()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(k):
+            step()
+        e1.record(stream)
+        e1.synchronize()
+        return adist.max_over_ranks(e0.elapsed_time(e1) / k)
+
+    for _ in range(args.warmup):
+        e.integrate_step()
+        e.integrate_step_sequential()
+    e.synchronize()
+    l0 = e.launch_count()
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        ms = timed(e.integrate_step, args.steps)
+    launches = e.launch_count() - l0
+    l1 = e.launch_count()
+    ms_seq = timed(e.integrate_step_sequential, args.steps)
+    launches_seq = e.launch_count() - l1
+    e.destroy()
+    peak, _ = peaks()
+    achieved = BYTES_PER_CELL_STEP["fp32comp"] * total_cells / world / (ms * 1e-3) / 1e9
+    return {"workload": "64 members, N in {32,48,64,96}, nu/eta log-U[1e-3,1e-2], "
+                        "seeds 100..163, FP32 compensated, dt=1e-3",
+            "members": len(members), "cells": total_cells, "value": total_cells / (ms * 1e-3),
+            "unit": UNIT, "ms_per_step": ms, "gpu_launches": launches,
+            "sequential": {"value": total_cells / (ms_seq * 1e-3), "ms_per_step": ms_seq,
+                           "gpu_launches": launches_seq},
+            "speedup_vs_sequential": ms_seq / ms, "tiles": list(tiles),
+            "autotune_solve_ms": tune_ms, "clocks": clk.summary(),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak,
+                         "bytes_per_cell_step": BYTES_PER_CELL_STEP["fp32comp"],
+                         "note": "whole step incl. halo fills"},
+            "scaling": "strong (64 members split across ranks)"}
+
+
+def ab_cells(info):
+    from astaroth_b200.device import dims
+    nx, ny, nz = dims(info)
+    return nx * ny * nz
+
+
+def load_fields_by_parts(ab, dev, info, seed):
+    """Loads the seeded initial condition with a solenoidal velocity one part at
+    a time (uu as three fields together, then each other field), so the host
+    holds at most three fields."""
+    import numpy as np
+    from astaroth_b200 import capi
+    C = capi.C
+    lib = capi.load()
+    nx, ny, nz = ab.device.dims(info)
+    shape = (nz + 6, ny + 6, nx + 6)
+
+    def mesh_of(bufs):
+        m = capi.AcMesh()
+        m.info = info
+        for q, b in bufs.items():
+            m.vertex_buffer[q] = b.ctypes.data_as(C.POINTER(C.c_double))
+        return m
+
+    bufs = {q: np.empty(shape) for q in (1, 2, 3)}
+    m = mesh_of(bufs)
+    if lib.acHostMeshSolenoidalModes(C.byref(m), seed, 64, 8, 1e-2) != 0:
+        raise RuntimeError("acHostMeshSolenoidalModes failed")
+    for q in bufs:
+        if lib.acDeviceLoadVertexBuffer(dev.handle, 0, m, q) != 0:
+            raise RuntimeError("acDeviceLoadVertexBuffer failed")
+    del bufs, m
+    for q in (0, 4, 5, 6, 7):
+        bufs = {q: np.empty(shape)}
+        m = mesh_of(bufs)
+        if lib.acHostMeshRandomizeSeeded(C.byref(m), seed, 1e-5, 1e-3, 1e-4) != 0:
+            raise RuntimeError("acHostMeshRandomizeSeeded failed")
+        if lib.acDeviceLoadVertexBuffer(dev.handle, 0, m, q) != 0:
+            raise RuntimeError("acDeviceLoadVertexBuffer failed")
+        del bufs, m
+    dev.synchronize()
+
+
+def diagnostics(dev):
+    out = {}
+    for q, name in enumerate(("lnrho", "uux", "uuy", "uuz", "ax", "ay", "az", "entropy")):
+        out[name] = [dev.reduce_scal("RTYPE_MAX", q), dev.reduce_scal("RTYPE_MIN", q),
+                     dev.reduce_scal("RTYPE_RMS", q)]
+    out["uu_rms"] = [dev.reduce_vec("RTYPE_RMS", 1, 2, 3)]
+    out["aa_rms"] = [dev.reduce_vec("RTYPE_RMS", 4, 5, 6)]
+    return out
+
+
+def run_cfl1024(args):
+    """1024^3 interior, FP32 compensated (about 149 GB on the device), u a
+    solenoidal sum of 64 Fourier modes (|k| <= 8, amplitude 1e-2), aa ~
+    N(0, 1e-4^2), lnrho and s ~ U(-1e-5, 1e-5), seed 3; 20 RK3 steps whose dt
+    comes from the on-device CFL maxima (Courant factors cdt = 0.4, cdtv = 0.3).
+    The same run in FP64 with the same dt sequence checks the diagnostics."""
+    import torch
+    import astaroth_b200 as ab
+
+    n, steps = (args.n if args.n != 512 else 1024), 20
+    torch.cuda.set_device(0)
+    res = {}
+    for prec in (1, 0):
+        info = ab.make_info(n, precision=prec, **ab.CONFIG_PARAMS)
+        dev = ab.Device(info)
+        t0 = time.perf_counter()
+        load_fields_by_parts(ab, dev, info, 3)
+        t_load = time.perf_counter() - t0
+        stream = torch.cuda.ExternalStream(dev.stream_handle(0))
+        free_b, total_b = torch.cuda.mem_get_info()
+        if prec == 1:
+            dev.calc_timestep()
+            dts = []
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        l0 = dev.launch_count()
+        with ClockSampler(0) as clk:
+            ev0.record(stream)
+            for s in range(steps):
+                if prec == 1:
+                    dt = dev.timestep()  # from the maxima of the last substep 2
+                    dts.append(dt)
+                else:
+                    dt = dts[s]
+                dev.integrate_step(dt)
+            ev1.record(stream)
+            ev1.synchronize()
+        ms = ev0.elapsed_time(ev1) / steps
+        res[prec] = {"ms_per_step": ms, "value": n ** 3 / (ms * 1e-3),
+                     "gpu_launches": dev.launch_count() - l0, "clocks": clk.summary(),
+                     "device_bytes_used": total_b - free_b, "load_s": t_load,
+                     "diagnostics": diagnostics(dev)}
+        dev.destroy()
+        del dev
+        torch.cuda.synchronize()
+    d32, d64 = res[1]["diagnostics"], res[0]["diagnostics"]
+    rel = {k: max(abs(a - b) / max(abs(b), 1e-300) for a, b in zip(d32[k], d64[k]))
+           for k in d32}
+    peak, _ = peaks()
+    achieved = BYTES_PER_CELL_STEP["fp32comp"] * n ** 3 / (res[1]["ms_per_step"] * 1e-3) / 1e9
+    line = {"metric": f"cell-updates/s per RK3 step at {n}^3 (FP32-compensated, adaptive CFL)",
+            "value": res[1]["value"], "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": 0,
+            "ms_per_step": res[1]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 (compensated hi/lo)",
+            "data": "synthetic (seed 3: solenoidal uu of 64 modes, |k|<=8, amplitude 1e-2; "
+                    "aa ~ N(0,1e-4^2); lnrho, s ~ U(-1e-5,1e-5))",
+            "config": {"workload": f"{n}^3 FP32-compensated, {steps} RK3 steps, dt from the "
+                                   "on-device CFL maxima each step (cdt=0.4, cdtv=0.3)",
+                       "n": n},
+            "dt": dts, "gpu_launches": res[1]["gpu_launches"], "clocks": res[1]["clocks"],
+            "device_bytes_used": res[1]["device_bytes_used"],
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "note": "whole step incl. halo fills and "
+                                                          "the per-step host read of dt"},
+            "fp64_same_dts": {"ms_per_step": res[0]["ms_per_step"], "value": res[0]["value"],
+                              "device_bytes_used": res[0]["device_bytes_used"]},
+            "diagnostics_rel_diff_vs_fp64": rel,
+            "diagnostics_max_rel_diff": max(rel.values())}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.workload == "cfl1024":
+        run_cfl1024(args)
+        return
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -192,3 +192,24 @@ def capi_dims(info):
     from astaroth_b200.device import dims
 
     return dims(info)
+
+
+def test_seeded_generator_one_field_at_a_time():
+    """Each field's values do not depend on the other buffers: generating one
+    field with the others NULL gives the field of the full generation."""
+    from astaroth_b200.device import empty_mesh, make_info, mesh_struct, seeded_mesh
+
+    info = make_info((10, 12, 9))
+    full = seeded_mesh(info, 5)
+    lib = capi.load()
+    for q in (0, 3, 7):
+        part = empty_mesh(info)
+        m = capi.AcMesh()
+        m.info = info
+        m.vertex_buffer[q] = part[q].ctypes.data_as(C.POINTER(C.c_double))
+        assert lib.acHostMeshRandomizeSeeded(C.byref(m), 5, 1e-5, 1e-3, 1e-4) == 0
+        assert np.array_equal(part[q], full[q])
+    # the solenoidal generator needs all three velocity buffers
+    m = mesh_struct(empty_mesh(info), info)
+    m.vertex_buffer[2] = C.POINTER(C.c_double)()
+    assert lib.acHostMeshSolenoidalModes(C.byref(m), 3, 8, 4, 1e-2) != 0
