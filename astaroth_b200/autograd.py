@@ -4,10 +4,11 @@ function of the initial fields and of nu, eta.
 Forward: N RK3 steps of the device integrator (acDeviceIntegrateStep), with a
 checkpoint of the state every k steps.  Backward: for each checkpoint segment,
 from the last to the first, the segment is integrated again from its
-checkpoint, keeping the three substep states f_0, f_1, f_2 of every step; then
-for each step (last first) the discrete adjoint substeps s = 2, 1, 0 are
-applied (acDeviceIntegrateSubstepAdjoint).  Every step is recomputed once.
-Memory: N/k checkpoints plus 3k substep states.
+checkpoint, keeping the three substep states f_0, f_1, f_2 of every step
+(acDeviceAdjointTapeForward); then for each step (last first) the discrete
+adjoint substeps s = 2, 1, 0 are applied (acDeviceAdjointTapeBackward, i.e.
+acDeviceIntegrateSubstepAdjoint about the taped states).  Every step is
+recomputed once.  Memory: N/k checkpoints plus 3k substep states.
 
 Tensors are (8, mz, my, mx) float64 on the GPU (halos included, as the host
 AcMesh).  The integration fills the halos itself, so gradients live on the
@@ -70,7 +71,7 @@ class _Integrate(torch.autograd.Function):
         out = dev.store_mesh_device(torch.empty_like(f0))
         torch.cuda.synchronize()
         ctx.dev, ctx.steps, ctx.dt, ctx.every, ctx.ckpts = dev, steps, dt, every, ckpts
-        ctx.nu, ctx.eta = float(nu), float(eta)
+        ctx.nu, ctx.eta, ctx.tape = float(nu), float(eta), tape
         return out
 
     @staticmethod
@@ -81,14 +82,19 @@ class _Integrate(torch.autograd.Function):
         lam = torch.zeros_like(grad_out)
         interior(lam).copy_(interior(grad_out))
         dev.load_adjoint(lam)
-        # substep states f_0, f_1, f_2 of every step of one segment; written and
-        # read only by the device's stream, so no per-transfer synchronisation
-        buf = [torch.empty_like(grad_out) for _ in range(3 * min(every, steps))]
         torch.cuda.synchronize()
         for seg in reversed(range(len(ctx.ckpts))):
             n0 = seg * every
             n1 = min(n0 + every, steps)
             dev.load_mesh_device(ctx.ckpts[seg], wait_torch=False)
+            if ctx.tape:
+                # the library keeps the segment's substep states on its own tape
+                dev.adjoint_tape_forward(n1 - n0, dt)
+                dev.adjoint_tape_backward(n1 - n0, dt)
+                continue
+            # the same sweep through the per-substep entry points, with the
+            # substep states f_0, f_1, f_2 of every step kept in torch tensors
+            buf = [torch.empty_like(grad_out) for _ in range(3 * (n1 - n0))]
             for n in range(n1 - n0):
                 for s in range(3):
                     dev.store_mesh_device(buf[3 * n + s], sync=False)
@@ -108,17 +114,21 @@ class _Integrate(torch.autograd.Function):
         nu_bar, eta_bar = dev.param_adjoints()
         dtype, device = grad_out.dtype, grad_out.device
         return (out, torch.tensor(nu_bar, dtype=dtype, device=device),
-                torch.tensor(eta_bar, dtype=dtype, device=device), None, None, None, None)
+                torch.tensor(eta_bar, dtype=dtype, device=device), None, None, None, None, None)
 
 
 def integrate(f0: torch.Tensor, nu, eta, dev: Device, steps: int, dt: float,
-              checkpoint_every: int | None = None) -> torch.Tensor:
+              checkpoint_every: int | None = None, tape: bool = True) -> torch.Tensor:
     """Differentiable N-step integration on `dev` (an FP64 Device of matching size).
 
     f0: (8, mz, my, mx) float64 CUDA tensor; nu, eta: 0-d tensors (may require grad).
     Returns the final state; backward gives d/d f0 (interior), d/d nu and d/d eta.
+    tape=True sweeps each segment with acDeviceAdjointTapeForward/Backward (the
+    library keeps the substep states); tape=False makes one call per substep
+    (acDevicePeriodicBoundconds + acDeviceIntegrateSubstepAdjoint) with the
+    states in torch tensors.  Both apply the same kernels in the same order.
     """
     every = checkpoint_every or max(1, int(math.sqrt(steps)))
     nu = torch.as_tensor(nu, dtype=torch.float64, device=f0.device)
     eta = torch.as_tensor(eta, dtype=torch.float64, device=f0.device)
-    return _Integrate.apply(f0, nu, eta, dev, steps, dt, every)
+    return _Integrate.apply(f0, nu, eta, dev, steps, dt, every, tape)

@@ -241,6 +241,8 @@ SIGNATURES = {
     "acDeviceStoreAdjoint": (C.c_int, [Device_p, C.c_int, C.POINTER(C.c_void_p)]),
     "acDeviceGetParamAdjoints": (C.c_int, [Device_p, C.POINTER(C.c_double),
                                            C.POINTER(C.c_double)]),
+    "acDeviceAdjointTapeForward": (C.c_int, [Device_p, C.c_int, C.c_int, C.c_double]),
+    "acDeviceAdjointTapeBackward": (C.c_int, [Device_p, C.c_int, C.c_int, C.c_double]),
     "acDeviceGetStreamHandle": (C.c_void_p, [Device_p, C.c_int]),
     "acDeviceGetLaunchCount": (C.c_ulonglong, [Device_p]),
     "acB200Version": (C.c_char_p, []),

@@ -177,6 +177,7 @@ release(Device d)
     cudaFree(d->adj_lw);
     cudaFree(d->adj_mu);
     cudaFree(d->adj_pgrad);
+    cudaFree(d->adj_tape);
     cudaFreeHost(d->host_result);
     for (int s = 0; s < NUM_STREAMS; ++s)
         if (d->streams[s])
@@ -1083,6 +1084,30 @@ acDeviceStoreAdjoint(const Device d, const Stream stream, AcReal* const* lam_f)
     return AC_SUCCESS;
 }
 
+/* One adjoint substep about the state `state` (8 fields at q * cells, halos
+ * filled), or about the in-buffers when state is NULL. */
+static cudaError_t
+launch_adjoint(const Device d, cudaStream_t st, const int step, const double dt,
+               const double* state)
+{
+    StencilCoef sc;
+    PhysConst pc;
+    ac_make_stencil(d->config, &sc);
+    ac_make_phys(d->config, &pc);
+    AdjointFields a;
+    for (int q = 0; q < AC_NF; ++q) {
+        a.f[q]  = state ? state + (size_t)q * d->geom.cells : arr64(d, d->in_idx[q], q);
+        a.lf[q] = d->adj_lf + (size_t)q * d->geom.cells;
+        a.lw[q] = d->adj_lw + (size_t)q * d->geom.cells;
+    }
+    for (int m = 0; m < AC_MU_COUNT; ++m)
+        a.mu[m] = d->adj_mu + (size_t)m * d->geom.cells;
+    const double alpha[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
+    const double beta[3]  = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
+    return ac_launch_adjoint_substep(d->geom, a, sc, pc, alpha[step], beta[step], dt,
+                                     d->adj_pgrad, st, &d->launches);
+}
+
 extern "C" AcResult
 acDeviceIntegrateSubstepAdjoint(const Device d, const Stream stream, const int step_number,
                                 const Volume start, const Volume end, const AcReal dt)
@@ -1094,23 +1119,63 @@ acDeviceIntegrateSubstepAdjoint(const Device d, const Stream stream, const int s
         return AC_FAILURE;
     }
     AC_CUDA_CHECK(cudaSetDevice(d->id));
-    StencilCoef sc;
-    PhysConst pc;
-    ac_make_stencil(d->config, &sc);
-    ac_make_phys(d->config, &pc);
-    AdjointFields a;
-    for (int q = 0; q < AC_NF; ++q) {
-        a.f[q]  = arr64(d, d->in_idx[q], q);
-        a.lf[q] = d->adj_lf + (size_t)q * d->geom.cells;
-        a.lw[q] = d->adj_lw + (size_t)q * d->geom.cells;
+    AC_CUDA_CHECK(launch_adjoint(d, d->streams[stream], step_number, dt, NULL));
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceAdjointTapeForward(const Device d, const Stream stream, const int steps, const AcReal dt)
+{
+    if (!d || !stream_ok(stream) || steps < 1)
+        return AC_FAILURE;
+    const int blk = in_block_index(d);
+    if (blk < 0) {
+        fprintf(stderr, "astaroth_b200: the tape needs every field's in-buffer in one block\n");
+        return AC_FAILURE;
     }
-    for (int m = 0; m < AC_MU_COUNT; ++m)
-        a.mu[m] = d->adj_mu + (size_t)m * d->geom.cells;
-    const double alpha[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
-    const double beta[3]  = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
-    AC_CUDA_CHECK(ac_launch_adjoint_substep(d->geom, a, sc, pc, alpha[step_number],
-                                            beta[step_number], dt, d->adj_pgrad,
-                                            d->streams[stream], &d->launches));
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    if (ensure_adjoint(d) != AC_SUCCESS)
+        return AC_FAILURE;
+    const size_t state_elems = (size_t)AC_NF * d->geom.cells;
+    if (d->adj_tape_states < 3 * steps) {
+        AC_CUDA_CHECK(cudaDeviceSynchronize());
+        cudaFree(d->adj_tape);
+        d->adj_tape        = NULL;
+        d->adj_tape_states = 0;
+        AC_CUDA_CHECK(cudaMalloc((void**)&d->adj_tape, 3 * (size_t)steps * state_elems *
+                                                           sizeof(double)));
+        d->adj_tape_states = 3 * steps;
+    }
+    cudaStream_t st = d->streams[stream];
+    const Volume m0 = {0, 0, 0};
+    const Volume m1 = {(size_t)d->geom.mx, (size_t)d->geom.my, (size_t)d->geom.mz};
+    for (int n = 0; n < steps; ++n)
+        for (int s = 0; s < 3; ++s) {
+            AC_CUDA_CHECK(launch_periodic(d, st, 0, AC_NF, m0, m1, &d->launches));
+            /* the 8 in-buffers are one contiguous block: one copy per state */
+            AC_CUDA_CHECK(cudaMemcpyAsync(d->adj_tape + (size_t)(3 * n + s) * state_elems,
+                                          arr64(d, d->in_idx[0], 0),
+                                          state_elems * sizeof(double),
+                                          cudaMemcpyDeviceToDevice, st));
+            AC_CUDA_CHECK(launch_substep(d, st, s, dt, &d->launches));
+            acDeviceSwapBuffers(d);
+        }
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceAdjointTapeBackward(const Device d, const Stream stream, const int steps,
+                            const AcReal dt)
+{
+    if (!d || !stream_ok(stream) || steps < 1 || !d->adj_lf || d->adj_tape_states < 3 * steps)
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    cudaStream_t st             = d->streams[stream];
+    const size_t state_elems    = (size_t)AC_NF * d->geom.cells;
+    for (int n = steps - 1; n >= 0; --n)
+        for (int s = 2; s >= 0; --s)
+            AC_CUDA_CHECK(launch_adjoint(d, st, s, dt,
+                                         d->adj_tape + (size_t)(3 * n + s) * state_elems));
     return AC_SUCCESS;
 }
 

@@ -159,6 +159,8 @@ struct device_s {
     double* adj_lw;      /* 8 fields */
     double* adj_mu;      /* AC_MU_COUNT fields */
     double* adj_pgrad;   /* 2 values: d/d nu, d/d eta */
+    double* adj_tape;    /* substep input states of a recomputed segment, 8 fields each */
+    int adj_tape_states; /* states the tape holds */
     unsigned long long launches;
 };
 

@@ -4,7 +4,8 @@
  * update works on (hi, lo) pairs, see rk_update_comp).
  *
  * Each CTA owns a 32 x 4 (x, y) tile of the interior and marches along z over
- * a chunk of ZCHUNK planes.  A ring of RING = 8 shared-memory slots holds the
+ * a chunk of up to ZCHUNK planes (fewer on small meshes, so that the grid
+ * still covers the SMs; see zchunk_for).  A ring of RING = 8 shared-memory slots holds the
  * planes z-3 .. z+3 the stencils of plane z need plus one plane in flight.
  * One TMA instruction (cp.async.bulk.tensor.4d, no multicast) brings a whole
  * plane of all 8 fields -- a (38 x 10 x 1 x 8) box of the in-buffer (40 wide
@@ -233,7 +234,7 @@ template <typename T, bool COMP>
 __global__ void __launch_bounds__(2 * TX * TY, Tile<T>::MINB)
 solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const FieldsT<T> f,
                    const StencilT<T> sc, const PhysConst pc, const RkCoef rk, int* err,
-                   unsigned long long* cfl)
+                   unsigned long long* cfl, const int zchunk)
 {
     typedef Layout<T> L;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -249,8 +250,8 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
     const int cell  = ly * TX + lx;
     const int x0    = blockIdx.x * TX;
     const int y0    = blockIdx.y * TY;
-    const int z0    = blockIdx.z * ZCHUNK;
-    const int z1    = min(z0 + ZCHUNK, g.nz);
+    const int z0    = blockIdx.z * zchunk;
+    const int z1    = min(z0 + zchunk, g.nz);
     const int pfirst = z0 - NGHOST;     /* first plane needed (interior z index) */
     const int plast  = z1 - 1 + NGHOST; /* last plane needed */
 
@@ -444,6 +445,19 @@ make_map(void* map_out, void* base, const Geom& g)
     return r == CUDA_SUCCESS;
 }
 
+/* Planes per CTA: ZCHUNK, halved (down to 8) while the grid would have fewer
+ * than two CTAs per SM of the 148.  Every chunk reads 6 halo planes beyond its
+ * own, so long chunks are cheaper where the grid is large enough. */
+int
+zchunk_for(const Geom& g)
+{
+    const long long tiles = (long long)((g.nx + TX - 1) / TX) * ((g.ny + TY - 1) / TY);
+    int zc                = ZCHUNK;
+    while (zc > 8 && tiles * ((g.nz + zc - 1) / zc) < 2 * 148)
+        zc /= 2;
+    return zc;
+}
+
 template <typename T, bool COMP>
 cudaError_t
 launch_tiled(const Geom& g, const void* tmap_in, const FieldsT<T>& f, const StencilCoef& sc,
@@ -451,9 +465,10 @@ launch_tiled(const Geom& g, const void* tmap_in, const FieldsT<T>& f, const Sten
              cudaStream_t stream, unsigned long long* launches)
 {
     const dim3 tpb(TX, 2 * TY, 1);
-    const dim3 bpg((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + ZCHUNK - 1) / ZCHUNK);
+    const int zc = zchunk_for(g);
+    const dim3 bpg((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + zc - 1) / zc);
     solve_tiled_kernel<T, COMP><<<bpg, tpb, Layout<T>::SMEM_BYTES, stream>>>(
-        *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err, cfl);
+        *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err, cfl, zc);
     if (launches)
         ++*launches;
     return cudaGetLastError();

@@ -292,6 +292,14 @@ class Device:
                                                         self.vols.n1, dt),
                "acDeviceIntegrateSubstepAdjoint")
 
+    def adjoint_tape_forward(self, steps: int, dt: float, stream: int = 0) -> None:
+        _check(self.lib.acDeviceAdjointTapeForward(self._h, stream, steps, dt),
+               "acDeviceAdjointTapeForward")
+
+    def adjoint_tape_backward(self, steps: int, dt: float, stream: int = 0) -> None:
+        _check(self.lib.acDeviceAdjointTapeBackward(self._h, stream, steps, dt),
+               "acDeviceAdjointTapeBackward")
+
     def param_adjoints(self):
         nu, eta = C.c_double(), C.c_double()
         _check(self.lib.acDeviceGetParamAdjoints(self._h, C.byref(nu), C.byref(eta)),

@@ -542,12 +542,26 @@ def diagnostics(dev):
     return out
 
 
+# Diffusive Courant factor of the 1024^3 run.  The timestep bound of the
+# reference (samples/standalone_mpi/main.cc:430-440, mhdsolver.ac:551-583) is
+# cdtv * dsmin^2 / max(nu, eta, gamma chi), with no dimension or stencil factor
+# and without the bulk viscosity zeta.  The fastest decaying mode of the
+# 6th-order Laplacian in 3-D has eigenvalue -18.13 / dx^2, and the longitudinal
+# velocity diffuses with (4/3) nu + zeta = 0.0167, so RK3 (stable for
+# dt * |lambda| <= 2.51 on the negative real axis) needs cdtv <= 0.0415 at
+# nu = 5e-3.  cdtv = 0.3 (config/astaroth.conf:46) gives dt * |lambda| = 18 at
+# 1024^3, where the diffusive bound is the smaller one, and the run overflows
+# in a few steps (in the reference's formula as in this one).
+CFL1024_CDTV = 0.04
+
+
 def run_cfl1024(args):
     """1024^3 interior, FP32 compensated (about 149 GB on the device), u a
     solenoidal sum of 64 Fourier modes (|k| <= 8, amplitude 1e-2), aa ~
     N(0, 1e-4^2), lnrho and s ~ U(-1e-5, 1e-5), seed 3; 20 RK3 steps whose dt
-    comes from the on-device CFL maxima (Courant factors cdt = 0.4, cdtv = 0.3).
-    The same run in FP64 with the same dt sequence checks the diagnostics."""
+    comes from the on-device CFL maxima (Courant factors cdt = 0.4 and
+    cdtv = CFL1024_CDTV).  The same run in FP64 with the same dt sequence checks
+    the diagnostics (max, min, rms of every field)."""
     import torch
     import astaroth_b200 as ab
 
@@ -555,7 +569,7 @@ def run_cfl1024(args):
     torch.cuda.set_device(0)
     res = {}
     for prec in (1, 0):
-        info = ab.make_info(n, precision=prec, **ab.CONFIG_PARAMS)
+        info = ab.make_info(n, precision=prec, cdtv=CFL1024_CDTV, **ab.CONFIG_PARAMS)
         dev = ab.Device(info)
         t0 = time.perf_counter()
         load_fields_by_parts(ab, dev, info, 3)
@@ -599,8 +613,8 @@ def run_cfl1024(args):
             "data": "synthetic (seed 3: solenoidal uu of 64 modes, |k|<=8, amplitude 1e-2; "
                     "aa ~ N(0,1e-4^2); lnrho, s ~ U(-1e-5,1e-5))",
             "config": {"workload": f"{n}^3 FP32-compensated, {steps} RK3 steps, dt from the "
-                                   "on-device CFL maxima each step (cdt=0.4, cdtv=0.3)",
-                       "n": n},
+                                   f"on-device CFL maxima each step (cdt=0.4, "
+                                   f"cdtv={CFL1024_CDTV})", "n": n},
             "dt": dts, "gpu_launches": res[1]["gpu_launches"], "clocks": res[1]["clocks"],
             "device_bytes_used": res[1]["device_bytes_used"],
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -608,6 +622,7 @@ def run_cfl1024(args):
                                                           "the per-step host read of dt"},
             "fp64_same_dts": {"ms_per_step": res[0]["ms_per_step"], "value": res[0]["value"],
                               "device_bytes_used": res[0]["device_bytes_used"]},
+            "diagnostics_fp32comp": d32, "diagnostics_fp64": d64,
             "diagnostics_rel_diff_vs_fp64": rel,
             "diagnostics_max_rel_diff": max(rel.values())}
     print(json.dumps(line), flush=True)

@@ -11,9 +11,10 @@ import numpy as np
 import pytest
 
 from astaroth_b200 import capi
-from astaroth_b200.device import AstarothError, Device, info_to_dict, make_info, seeded_mesh
-from oracle import oracle
+from astaroth_b200.device import (AstarothError, Device, info_to_dict, make_info, mesh_struct,
+                                  seeded_mesh)
 from astaroth_b200.ensemble import Ensemble, ensemble_members
+from oracle import oracle
 
 pytestmark = pytest.mark.gpu
 
@@ -142,8 +143,9 @@ def test_errors():
         assert e.lib.acEnsembleLoadMember(e._h, -1, out) != capi.AC_SUCCESS
         with pytest.raises(AstarothError):
             e.set_tiles(7, 3, 4)  # 21 threads: not a multiple of 32
-        with pytest.raises(AstarothError):
-            e.load_member(0, seeded_mesh(make_info(48, precision=1), 1))  # wrong size
+        info48 = make_info(48, precision=1)  # a host mesh of the wrong size
+        wrong = mesh_struct(seeded_mesh(info48, 1), info48)
+        assert e.lib.acEnsembleLoadMember(e._h, 0, wrong) != capi.AC_SUCCESS
         with pytest.raises(AstarothError):
             e.reduce_scal(0, "RTYPE_ALFVEN_MAX", 0)
     with pytest.raises(AstarothError):
