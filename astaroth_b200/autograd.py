@@ -59,7 +59,7 @@ def energy(fields: torch.Tensor, info) -> torch.Tensor:
 
 class _Integrate(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, f0, nu, eta, dev, steps, dt, every):
+    def forward(ctx, f0, nu, eta, dev, steps, dt, every, tape):
         dev.set_real(capi.RealParam.AC_nu_visc, float(nu))
         dev.set_real(capi.RealParam.AC_eta, float(eta))
         dev.load_mesh_device(f0.contiguous())
