@@ -107,7 +107,7 @@ def test_gradient_matches_cpu_reference():
 
 def test_tape_sweep_equals_per_substep_sweep():
     """acDeviceAdjointTapeForward/Backward and the per-substep entry points
-    apply the same kernels in the same order: identical gradients."""
+    apply the same kernels in the same order: identical field gradients."""
     torch = _torch()
     from astaroth_b200 import autograd as AG
     info, f = mesh((24, 20, 16), 33)
@@ -122,7 +122,9 @@ def test_tape_sweep_equals_per_substep_sweep():
             AG.energy(fN, info).backward()
         grads.append((f0.grad.cpu().numpy(), float(nu.grad), float(eta.grad)))
     assert np.array_equal(grads[0][0], grads[1][0])
-    assert grads[0][1:] == grads[1][1:]
+    # the parameter adjoints are sums of per-block atomics, whose order varies
+    for a, b in zip(grads[0][1:], grads[1][1:]):
+        assert abs(a - b) <= 1e-12 * abs(b)
 
 
 def test_config4_fd_dot_product_and_cost():
