@@ -12,17 +12,24 @@
  *     lw <- alpha_s lw
  * and accumulates d/d(nu, eta) of dt lw . R.  J_R^T is applied in two
  * passes: adj_local_kernel evaluates, per cell, the reverse of the RHS into the
- * adjoints mu of the 46 derivative slots (mhd_rhs_adjoint.cuh); after a
- * periodic halo fill of mu, adj_gather_kernel applies the transposed stencils:
- * first derivatives are antisymmetric (D^T = -D), second, Laplacian and the
- * diagonal mixed stencils are symmetric, so the gather for a vector field is
- * value - div-like first-derivative terms + lap + grad div of the slot fields.
+ * adjoints mu of the 46 derivative slots (mhd_rhs_adjoint.cuh), adds the 8
+ * value slots to lf directly and stores the 38 others; adj_gather_kernel then
+ * applies the transposed stencils at wrapped (periodic) interior indices, so
+ * mu needs no halo fill: first derivatives are antisymmetric (D^T = -D),
+ * second, Laplacian and the diagonal mixed stencils are symmetric, so the
+ * gather for a vector field is - div-like first-derivative terms + lap + grad
+ * div of the slot fields.  The gather runs one output field per block.
  */
 #include "internal.h"
 #include "mhd_rhs_adjoint.cuh"
 #include "stencil_plain.cuh"
 
 namespace {
+
+/* z planes per thread of the gather: consecutive planes of one column share
+ * most stencil taps, which then come from L1.  (The local kernel keeps one
+ * plane per thread: a loop there spills its 254 registers.) */
+constexpr int KZ = 4;
 
 __global__ void __launch_bounds__(128)
 adj_local_kernel(const Geom g, const AdjointFields a, const StencilCoef sc, const PhysConst pc,
@@ -58,9 +65,21 @@ adj_local_kernel(const Geom g, const AdjointFields a, const StencilCoef sc, cons
         /* the rate order of mhd_rates: lnrho, ux, uy, uz, ax, ay, az, entropy */
         double mu[MU_COUNT];
         mhd_rates_adjoint(L, S, U, A, phys_cast<double>(pc), lam, mu, gnu, geta);
+        /* value slots need no stencil: their transpose is the identity */
+        const int vslot[AC_NF] = {MU_L + MU_SV,     MU_U + MU_VV,     MU_U + MU_VV + 1,
+                                  MU_U + MU_VV + 2, MU_A + MU_VV,     MU_A + MU_VV + 1,
+                                  MU_A + MU_VV + 2, MU_S + MU_SV};
 #pragma unroll
-        for (int m = 0; m < MU_COUNT; ++m)
-            a.mu[m][idx] = mu[m];
+        for (int q = 0; q < AC_NF; ++q)
+            a.lf[q][idx] += mu[vslot[q]];
+#pragma unroll
+        for (int m = 0; m < MU_COUNT; ++m) {
+            const bool value_slot = m == MU_L + MU_SV || m == MU_S + MU_SV ||
+                                    (m >= MU_U + MU_VV && m < MU_U + MU_VV + 3) ||
+                                    (m >= MU_A + MU_VV && m < MU_A + MU_VV + 3);
+            if (!value_slot)
+                a.mu[m][idx] = mu[m];
+        }
     }
     /* block sums of the parameter adjoints, one atomic per block and value */
     const int tid = threadIdx.y * blockDim.x + threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -85,69 +104,137 @@ adj_local_kernel(const Geom g, const AdjointFields a, const StencilCoef sc, cons
     }
 }
 
-/* lap of a slot field at idx */
-__device__ __forceinline__ double
-lap_of(const double* f, const long long* st, const StencilCoef& sc)
+/* Periodic neighbour offsets of one interior cell: o[a][d + 3] is the index
+ * offset of the interior cell d steps away along axis a, wrapped.  The slot
+ * arrays mu are read only at interior cells, so they need no halo fill. */
+struct Wrap {
+    long long o[3][7];
+};
+
+__device__ __forceinline__ int
+wrap(const int v, const int n)
 {
-    return (sc.d2[0][0] + sc.d2[1][0] + sc.d2[2][0]) * __ldg(f) + der2_sides(f, st[0], sc.d2[0]) +
-           der2_sides(f, st[1], sc.d2[1]) + der2_sides(f, st[2], sc.d2[2]);
+    const int r = v % n;
+    return r < 0 ? r + n : r;
 }
 
-/* value + sum_a D_a^T g_a + lap^T lap for a scalar slot block at base m */
-__device__ __forceinline__ double
-gather_scalar(const AdjointFields& a, const int m, const long long idx, const long long* st,
-              const StencilCoef& sc)
-{
-    double acc = __ldg(a.mu[m + MU_SV] + idx);
-#pragma unroll
-    for (int ax = 0; ax < 3; ++ax)
-        acc -= der1(a.mu[m + MU_SG + ax] + idx, st[ax], sc.d1[ax]);
-    return acc + lap_of(a.mu[m + MU_SLAP] + idx, st, sc);
-}
-
-/* the same for component c of a vector slot block, plus grad div^T = grad div of
- * the three gd slots */
 __device__ __forceinline__ void
-gather_vector(const AdjointFields& a, const int m, const long long idx, const long long* st,
-              const StencilCoef& sc, double out[3])
+make_wrap(const Geom& g, const int i, const int j, const int k, Wrap& w)
 {
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        double acc = __ldg(a.mu[m + MU_VV + c] + idx);
-#pragma unroll
-        for (int ax = 0; ax < 3; ++ax)
-            acc -= der1(a.mu[m + MU_VG + 3 * c + ax] + idx, st[ax], sc.d1[ax]);
-        out[c] = acc + lap_of(a.mu[m + MU_VLAP + c] + idx, st, sc);
+    for (int d = -3; d <= 3; ++d) {
+        w.o[0][d + 3] = (long long)(wrap(i + d, g.nx) - i);
+        w.o[1][d + 3] = (long long)(wrap(j + d, g.ny) - j) * g.px;
+        w.o[2][d + 3] = (long long)(wrap(k + d, g.nz) - k) * g.pxy;
     }
-    const double* gd0 = a.mu[m + MU_VGD + 0] + idx;
-    const double* gd1 = a.mu[m + MU_VGD + 1] + idx;
-    const double* gd2 = a.mu[m + MU_VGD + 2] + idx;
-    const double d00  = sc.d2[0][0] * __ldg(gd0) + der2_sides(gd0, st[0], sc.d2[0]);
-    const double d11  = sc.d2[1][0] * __ldg(gd1) + der2_sides(gd1, st[1], sc.d2[1]);
-    const double d22  = sc.d2[2][0] * __ldg(gd2) + der2_sides(gd2, st[2], sc.d2[2]);
-    out[0] += d00 + dermix(gd1, st[0], st[1], sc.mix[0]) + dermix(gd2, st[0], st[2], sc.mix[1]);
-    out[1] += dermix(gd0, st[0], st[1], sc.mix[0]) + d11 + dermix(gd2, st[1], st[2], sc.mix[2]);
-    out[2] += dermix(gd0, st[0], st[2], sc.mix[1]) + dermix(gd1, st[1], st[2], sc.mix[2]) + d22;
 }
 
+/* sum_k c_k (f[+k] - f[-k]) along axis A */
+template <int A>
+__device__ __forceinline__ double
+wd1(const double* f, const Wrap& w, const double* c)
+{
+    double r = c[0] * (__ldg(f + w.o[A][4]) - __ldg(f + w.o[A][2]));
+    r        = fma(c[1], __ldg(f + w.o[A][5]) - __ldg(f + w.o[A][1]), r);
+    r        = fma(c[2], __ldg(f + w.o[A][6]) - __ldg(f + w.o[A][0]), r);
+    return r;
+}
+
+/* sum_k d_k (f[+k] + f[-k]) along axis A (centre excluded) */
+template <int A>
+__device__ __forceinline__ double
+wd2s(const double* f, const Wrap& w, const double* d)
+{
+    double r = d[1] * (__ldg(f + w.o[A][4]) + __ldg(f + w.o[A][2]));
+    r        = fma(d[2], __ldg(f + w.o[A][5]) + __ldg(f + w.o[A][1]), r);
+    r        = fma(d[3], __ldg(f + w.o[A][6]) + __ldg(f + w.o[A][0]), r);
+    return r;
+}
+
+/* sum_k e_k (f(+k,+k) + f(-k,-k) - f(+k,-k) - f(-k,+k)) along axes A, B */
+template <int A, int B>
+__device__ __forceinline__ double
+wmix(const double* f, const Wrap& w, const double* e)
+{
+    double r = 0;
+#pragma unroll
+    for (int k = 1; k <= 3; ++k) {
+        const double t = (__ldg(f + w.o[A][3 + k] + w.o[B][3 + k]) +
+                          __ldg(f + w.o[A][3 - k] + w.o[B][3 - k])) -
+                         (__ldg(f + w.o[A][3 + k] + w.o[B][3 - k]) +
+                          __ldg(f + w.o[A][3 - k] + w.o[B][3 + k]));
+        r = k == 1 ? e[0] * t : fma(e[k - 1], t, r);
+    }
+    return r;
+}
+
+__device__ __forceinline__ double
+wlap(const double* f, const Wrap& w, const StencilCoef& sc)
+{
+    return (sc.d2[0][0] + sc.d2[1][0] + sc.d2[2][0]) * __ldg(f) + wd2s<0>(f, w, sc.d2[0]) +
+           wd2s<1>(f, w, sc.d2[1]) + wd2s<2>(f, w, sc.d2[2]);
+}
+
+/* - sum_a D_a g_a + lap(l): the transposed first-derivative and Laplacian
+ * terms of one output field (D1^T = -D1, the Laplacian is symmetric) */
+__device__ __forceinline__ double
+gather_gl(const AdjointFields& a, const int g0, const int l, const long long idx, const Wrap& w,
+          const StencilCoef& sc)
+{
+    double acc = -wd1<0>(a.mu[g0] + idx, w, sc.d1[0]);
+    acc -= wd1<1>(a.mu[g0 + 1] + idx, w, sc.d1[1]);
+    acc -= wd1<2>(a.mu[g0 + 2] + idx, w, sc.d1[2]);
+    return acc + wlap(a.mu[l] + idx, w, sc);
+}
+
+/* (grad div)^T = grad div of the three gd slots, component C */
+template <int C>
+__device__ __forceinline__ double
+gather_gd(const AdjointFields& a, const int gd0, const long long idx, const Wrap& w,
+          const StencilCoef& sc)
+{
+    const double* g0 = a.mu[gd0] + idx;
+    const double* g1 = a.mu[gd0 + 1] + idx;
+    const double* g2 = a.mu[gd0 + 2] + idx;
+    if (C == 0)
+        return (sc.d2[0][0] * __ldg(g0) + wd2s<0>(g0, w, sc.d2[0])) +
+               wmix<0, 1>(g1, w, sc.mix[0]) + wmix<0, 2>(g2, w, sc.mix[1]);
+    if (C == 1)
+        return wmix<0, 1>(g0, w, sc.mix[0]) + (sc.d2[1][0] * __ldg(g1) + wd2s<1>(g1, w, sc.d2[1])) +
+               wmix<1, 2>(g2, w, sc.mix[2]);
+    return wmix<0, 2>(g0, w, sc.mix[1]) + wmix<1, 2>(g1, w, sc.mix[2]) +
+           (sc.d2[2][0] * __ldg(g2) + wd2s<2>(g2, w, sc.d2[2]));
+}
+
+/* One output field per block (blockIdx.z = zblock * AC_NF + q), so a block
+ * reads only the slot arrays of that field; KZ planes per thread. */
 __global__ void __launch_bounds__(128)
 adj_gather_kernel(const Geom g, const AdjointFields a, const StencilCoef sc, const double alpha)
 {
     const int i = threadIdx.x + blockIdx.x * blockDim.x;
     const int j = threadIdx.y + blockIdx.y * blockDim.y;
-    const int k = blockIdx.z;
-    if (i >= g.nx || j >= g.ny || k >= g.nz)
+    const int q = blockIdx.z % AC_NF;
+    if (i >= g.nx || j >= g.ny)
         return;
-    const long long idx   = geom_idx(g, i + NGHOST, j + NGHOST, k + NGHOST);
-    const long long st[3] = {1, (long long)g.px, g.pxy};
-    double add[AC_NF];
-    add[VTXBUF_LNRHO]   = gather_scalar(a, MU_L, idx, st, sc);
-    add[VTXBUF_ENTROPY] = gather_scalar(a, MU_S, idx, st, sc);
-    gather_vector(a, MU_U, idx, st, sc, &add[VTXBUF_UUX]);
-    gather_vector(a, MU_A, idx, st, sc, &add[VTXBUF_AX]);
-#pragma unroll
-    for (int q = 0; q < AC_NF; ++q) {
-        a.lf[q][idx] += add[q];
+    const int k1 = min((int)(blockIdx.z / AC_NF + 1) * KZ, g.nz);
+    for (int k = blockIdx.z / AC_NF * KZ; k < k1; ++k) {
+        const long long idx = geom_idx(g, i + NGHOST, j + NGHOST, k + NGHOST);
+        Wrap w;
+        make_wrap(g, i, j, k, w);
+        double add;
+        if (q == VTXBUF_LNRHO || q == VTXBUF_ENTROPY) {
+            const int m = q == VTXBUF_LNRHO ? MU_L : MU_S;
+            add         = gather_gl(a, m + MU_SG, m + MU_SLAP, idx, w, sc);
+        }
+        else {
+            const int m = q <= VTXBUF_UUZ ? MU_U : MU_A;
+            const int c = q <= VTXBUF_UUZ ? q - VTXBUF_UUX : q - VTXBUF_AX;
+            add         = gather_gl(a, m + MU_VG + 3 * c, m + MU_VLAP + c, idx, w, sc);
+            add += c == 0 ? gather_gd<0>(a, m + MU_VGD, idx, w, sc)
+                          : c == 1 ? gather_gd<1>(a, m + MU_VGD, idx, w, sc)
+                                   : gather_gd<2>(a, m + MU_VGD, idx, w, sc);
+        }
+        a.lf[q][idx] += add;
         a.lw[q][idx] *= alpha;
     }
 }
@@ -166,12 +253,11 @@ ac_launch_adjoint_substep(const Geom& g, const AdjointFields& a, const StencilCo
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess)
         return e;
-    const Volume m0 = {0, 0, 0};
-    const Volume m1 = {(size_t)g.mx, (size_t)g.my, (size_t)g.mz};
-    e = ac_launch_periodic<double>(g, a.mu, MU_COUNT, m0, m1, stream, launches);
-    if (e != cudaSuccess)
-        return e;
-    adj_gather_kernel<<<bpg, tpb, 0, stream>>>(g, a, sc, alpha);
+    const unsigned zb = (unsigned)((g.nz + KZ - 1) / KZ);
+    if ((long long)zb * AC_NF > 65535)
+        return cudaErrorInvalidConfiguration;
+    const dim3 gpg(bpg.x, bpg.y, zb * AC_NF);
+    adj_gather_kernel<<<gpg, tpb, 0, stream>>>(g, a, sc, alpha);
     if (launches)
         *launches += 2;
     return cudaGetLastError();

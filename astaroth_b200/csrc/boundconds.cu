@@ -124,6 +124,15 @@ join_kernel(const Geom g, const float* __restrict__ hi, const float* __restrict_
     }
 }
 
+/* dst = src for n2 double2 pairs (both 16-byte aligned), grid-stride */
+__global__ void
+copy2_kernel(const double2* __restrict__ src, double2* __restrict__ dst, const long long n2)
+{
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n2;
+         t += (long long)gridDim.x * blockDim.x)
+        dst[t] = src[t];
+}
+
 int
 grid_for(const long long work, const int tpb)
 {
@@ -200,6 +209,22 @@ ac_launch_fill_comp(float* hi, float* lo, const long long count, const double va
     const float h = (float)value;
     const float l = (float)(value - (double)h);
     fill_comp_kernel<<<grid_for(count, 256), 256, 0, stream>>>(hi, lo, count, h, l);
+    if (launches)
+        ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t
+ac_launch_copy(const double* src, double* dst, const long long count, cudaStream_t stream,
+               unsigned long long* launches)
+{
+    if (count <= 0)
+        return cudaSuccess;
+    if ((count & 1) || ((uintptr_t)src & 15) || ((uintptr_t)dst & 15))
+        return cudaMemcpyAsync(dst, src, count * sizeof(double), cudaMemcpyDeviceToDevice,
+                               stream);
+    copy2_kernel<<<grid_for(count / 2, 256), 256, 0, stream>>>((const double2*)src,
+                                                              (double2*)dst, count / 2);
     if (launches)
         ++*launches;
     return cudaGetLastError();

@@ -1153,10 +1153,9 @@ acDeviceAdjointTapeForward(const Device d, const Stream stream, const int steps,
         for (int s = 0; s < 3; ++s) {
             AC_CUDA_CHECK(launch_periodic(d, st, 0, AC_NF, m0, m1, &d->launches));
             /* the 8 in-buffers are one contiguous block: one copy per state */
-            AC_CUDA_CHECK(cudaMemcpyAsync(d->adj_tape + (size_t)(3 * n + s) * state_elems,
-                                          arr64(d, d->in_idx[0], 0),
-                                          state_elems * sizeof(double),
-                                          cudaMemcpyDeviceToDevice, st));
+            AC_CUDA_CHECK(ac_launch_copy(arr64(d, d->in_idx[0], 0),
+                                         d->adj_tape + (size_t)(3 * n + s) * state_elems,
+                                         (long long)state_elems, st, &d->launches));
             AC_CUDA_CHECK(launch_substep(d, st, s, dt, &d->launches));
             acDeviceSwapBuffers(d);
         }

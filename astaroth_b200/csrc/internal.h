@@ -174,6 +174,10 @@ cudaError_t ac_launch_periodic(const Geom& g, T* const* arrays, const int n, con
 
 cudaError_t ac_launch_fill(double* ptr, const long long count, const double value,
                            cudaStream_t stream, unsigned long long* launches);
+/* dst = src for `count` doubles on the device (a vectorised copy kernel when
+ * both are 16-byte aligned and count is even, else cudaMemcpyAsync) */
+cudaError_t ac_launch_copy(const double* src, double* dst, const long long count,
+                           cudaStream_t stream, unsigned long long* launches);
 /* FP32 compensated: hi/lo of `count` elements from a double value */
 cudaError_t ac_launch_fill_comp(float* hi, float* lo, const long long count, const double value,
                                 cudaStream_t stream, unsigned long long* launches);
