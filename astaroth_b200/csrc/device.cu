@@ -149,8 +149,17 @@ stream_ok(const Stream s)
 }
 
 static void
+invalidate_tape_graph(Device d)
+{
+    if (d->tape_valid)
+        cudaGraphExecDestroy(d->tape_exec);
+    d->tape_valid = 0;
+}
+
+static void
 invalidate_graphs(Device d)
 {
+    invalidate_tape_graph(d);
     for (int s = 0; s < NUM_STREAMS; ++s)
         for (int p = 0; p < 2; ++p) {
             if (d->graphs[s][p].valid)
@@ -1123,6 +1132,33 @@ acDeviceIntegrateSubstepAdjoint(const Device d, const Stream stream, const int s
     return AC_SUCCESS;
 }
 
+/* The launches of a tape recompute: per substep, halo fill, copy of the
+ * in-block to the tape, substep, swap. */
+static cudaError_t
+record_tape(Device d, cudaStream_t st, const int steps, const double dt)
+{
+    const size_t state_elems = (size_t)AC_NF * d->geom.cells;
+    const Volume m0          = {0, 0, 0};
+    const Volume m1          = {(size_t)d->geom.mx, (size_t)d->geom.my, (size_t)d->geom.mz};
+    for (int n = 0; n < steps; ++n)
+        for (int s = 0; s < 3; ++s) {
+            cudaError_t e = launch_periodic(d, st, 0, AC_NF, m0, m1, NULL);
+            if (e != cudaSuccess)
+                return e;
+            /* the 8 in-buffers are one contiguous block: one copy per state */
+            e = ac_launch_copy(arr64(d, d->in_idx[0], 0),
+                               d->adj_tape + (size_t)(3 * n + s) * state_elems,
+                               (long long)state_elems, st, NULL);
+            if (e != cudaSuccess)
+                return e;
+            e = launch_substep(d, st, s, dt, NULL);
+            if (e != cudaSuccess)
+                return e;
+            acDeviceSwapBuffers(d);
+        }
+    return cudaSuccess;
+}
+
 extern "C" AcResult
 acDeviceAdjointTapeForward(const Device d, const Stream stream, const int steps, const AcReal dt)
 {
@@ -1139,6 +1175,7 @@ acDeviceAdjointTapeForward(const Device d, const Stream stream, const int steps,
     const size_t state_elems = (size_t)AC_NF * d->geom.cells;
     if (d->adj_tape_states < 3 * steps) {
         AC_CUDA_CHECK(cudaDeviceSynchronize());
+        invalidate_tape_graph(d);
         cudaFree(d->adj_tape);
         d->adj_tape        = NULL;
         d->adj_tape_states = 0;
@@ -1147,18 +1184,32 @@ acDeviceAdjointTapeForward(const Device d, const Stream stream, const int steps,
         d->adj_tape_states = 3 * steps;
     }
     cudaStream_t st = d->streams[stream];
-    const Volume m0 = {0, 0, 0};
-    const Volume m1 = {(size_t)d->geom.mx, (size_t)d->geom.my, (size_t)d->geom.mz};
-    for (int n = 0; n < steps; ++n)
-        for (int s = 0; s < 3; ++s) {
-            AC_CUDA_CHECK(launch_periodic(d, st, 0, AC_NF, m0, m1, &d->launches));
-            /* the 8 in-buffers are one contiguous block: one copy per state */
-            AC_CUDA_CHECK(ac_launch_copy(arr64(d, d->in_idx[0], 0),
-                                         d->adj_tape + (size_t)(3 * n + s) * state_elems,
-                                         (long long)state_elems, st, &d->launches));
-            AC_CUDA_CHECK(launch_substep(d, st, s, dt, &d->launches));
-            acDeviceSwapBuffers(d);
-        }
+    /* the recompute is one CUDA graph, kept for the next call with the same
+     * steps, dt, in-block and stream (one per checkpoint segment) */
+    if (!(d->tape_valid && d->tape_steps == steps && d->tape_dt == dt && d->tape_blk == blk &&
+          d->tape_stream == (int)stream)) {
+        invalidate_tape_graph(d);
+        cudaGraph_t graph;
+        AC_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+        const cudaError_t rec = record_tape(d, st, steps, dt);
+        const cudaError_t end = cudaStreamEndCapture(st, &graph);
+        for (int q = 0; q < AC_NF; ++q) /* undo the capture's swaps */
+            d->in_idx[q] = blk;
+        AC_CUDA_CHECK(rec);
+        AC_CUDA_CHECK(end);
+        const cudaError_t inst = cudaGraphInstantiate(&d->tape_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        AC_CUDA_CHECK(inst);
+        d->tape_valid  = 1;
+        d->tape_steps  = steps;
+        d->tape_dt     = dt;
+        d->tape_blk    = blk;
+        d->tape_stream = (int)stream;
+    }
+    AC_CUDA_CHECK(cudaGraphLaunch(d->tape_exec, st));
+    d->launches += 9ull * steps;
+    if ((3 * steps) & 1) /* three swaps per step */
+        acDeviceSwapBuffers(d);
     return AC_SUCCESS;
 }
 

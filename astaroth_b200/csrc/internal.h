@@ -161,6 +161,10 @@ struct device_s {
     double* adj_pgrad;   /* 2 values: d/d nu, d/d eta */
     double* adj_tape;    /* substep input states of a recomputed segment, 8 fields each */
     int adj_tape_states; /* states the tape holds */
+    /* graph of the last acDeviceAdjointTapeForward (steps, dt, in-block, stream) */
+    cudaGraphExec_t tape_exec;
+    int tape_valid, tape_steps, tape_blk, tape_stream;
+    double tape_dt;
     unsigned long long launches;
 };
 
