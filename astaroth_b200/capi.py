@@ -241,6 +241,10 @@ SIGNATURES = {
     "acDeviceStoreAdjoint": (C.c_int, [Device_p, C.c_int, C.POINTER(C.c_void_p)]),
     "acDeviceGetParamAdjoints": (C.c_int, [Device_p, C.POINTER(C.c_double),
                                            C.POINTER(C.c_double)]),
+    "acHostMeshWriteToFile": (C.c_int, [AcMesh, C.c_size_t]),
+    "acHostMeshReadFromFile": (C.c_int, [C.c_size_t, C.POINTER(AcMesh)]),
+    "acDeviceWriteMeshToDisk": (C.c_int, [Device_p, C.c_char_p, C.c_char_p, C.c_int]),
+    "acDeviceReadMeshFromDisk": (C.c_int, [Device_p, C.c_char_p, C.c_char_p, C.c_int]),
     "acDeviceAdjointTapeForward": (C.c_int, [Device_p, C.c_int, C.c_int, C.c_double]),
     "acDeviceAdjointTapeBackward": (C.c_int, [Device_p, C.c_int, C.c_int, C.c_double]),
     "acDeviceGetStreamHandle": (C.c_void_p, [Device_p, C.c_int]),

@@ -17,6 +17,9 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <errno.h>
+#include <sys/stat.h>
+
 #include "internal.h"
 
 static const char* kVersion = "astaroth_b200 0.1 (sm_100a)";
@@ -1242,6 +1245,129 @@ acDeviceGetParamAdjoints(const Device d, AcReal* nu_bar, AcReal* eta_bar)
     *nu_bar  = v[0];
     *eta_bar = v[1];
     return AC_SUCCESS;
+}
+
+/* ---- snapshots of the computational domain: src/core/grid.cc:3792-3935 ----
+ * One raw file per field holding the interior nx*ny*nz values (x fastest):
+ * <dir>/<field name>-<label>.mesh, or with `segmented`,
+ * <dir>/<field name>-segment-<ox>-<oy>-<oz>-<label>.mesh where (ox, oy, oz) is
+ * AC_multigpu_offset ((0, 0, 0) on one GPU), the names the reference's grid
+ * layer writes without and with distributed I/O.  FP32-compensated meshes are
+ * written as the double values hi + lo. */
+static const char* const kSnapNames[NUM_VTXBUF_HANDLES] = {
+    "VTXBUF_LNRHO", "VTXBUF_UUX", "VTXBUF_UUY", "VTXBUF_UUZ",
+    "VTXBUF_AX",    "VTXBUF_AY",  "VTXBUF_AZ",  "VTXBUF_ENTROPY"};
+
+static bool
+snapshot_path(const Device d, const char* dir, const char* label, const int segmented,
+              const int q, char* out, const size_t len)
+{
+    const int3 o = d->config.int3_params[AC_multigpu_offset];
+    const int n  = segmented ? snprintf(out, len, "%s/%s-segment-%d-%d-%d-%s.mesh", dir,
+                                        kSnapNames[q], o.x, o.y, o.z, label)
+                             : snprintf(out, len, "%s/%s-%s.mesh", dir, kSnapNames[q], label);
+    return n >= 0 && (size_t)n < len;
+}
+
+extern "C" AcResult
+acDeviceWriteMeshToDisk(const Device d, const char* dir, const char* label, const int segmented)
+{
+    if (!d || !dir || !label)
+        return AC_FAILURE;
+    if (mkdir(dir, 0755) != 0 && errno != EEXIST) {
+        fprintf(stderr, "astaroth_b200: cannot create %s\n", dir);
+        return AC_FAILURE;
+    }
+    const Geom& g   = d->geom;
+    const size_t nm = (size_t)g.mx * g.my * g.mz;
+    double* buf     = (double*)malloc(nm * sizeof(double));
+    if (!buf)
+        return AC_FAILURE;
+    AcResult res = AC_SUCCESS;
+    for (int q = 0; q < AC_NF && res == AC_SUCCESS; ++q) {
+        AcMesh m;
+        memset(&m, 0, sizeof(m));
+        m.info            = d->config;
+        m.vertex_buffer[q] = buf;
+        res = acDeviceStoreVertexBuffer(d, STREAM_DEFAULT, (VertexBufferHandle)q, &m);
+        if (res != AC_SUCCESS)
+            break;
+        char path[4096];
+        FILE* fp = NULL;
+        if (!snapshot_path(d, dir, label, segmented, q, path, sizeof(path)) ||
+            !(fp = fopen(path, "wb"))) {
+            res = AC_FAILURE;
+            break;
+        }
+        for (int k = 0; k < g.nz && res == AC_SUCCESS; ++k)
+            for (int j = 0; j < g.ny; ++j) {
+                const double* row = buf + NGHOST + (size_t)g.mx * ((j + NGHOST) +
+                                                                  (size_t)g.my * (k + NGHOST));
+                if (fwrite(row, sizeof(double), g.nx, fp) != (size_t)g.nx) {
+                    res = AC_FAILURE;
+                    break;
+                }
+            }
+        if (fclose(fp) != 0)
+            res = AC_FAILURE;
+    }
+    free(buf);
+    return res;
+}
+
+extern "C" AcResult
+acDeviceReadMeshFromDisk(const Device d, const char* dir, const char* label, const int segmented)
+{
+    if (!d || !dir || !label)
+        return AC_FAILURE;
+    const Geom& g   = d->geom;
+    const size_t nm = (size_t)g.mx * g.my * g.mz;
+    double* buf     = (double*)calloc(nm, sizeof(double));
+    if (!buf)
+        return AC_FAILURE;
+    AcResult res = AC_SUCCESS;
+    for (int q = 0; q < AC_NF && res == AC_SUCCESS; ++q) {
+        char path[4096];
+        FILE* fp = NULL;
+        if (!snapshot_path(d, dir, label, segmented, q, path, sizeof(path)) ||
+            !(fp = fopen(path, "rb"))) {
+            fprintf(stderr, "astaroth_b200: cannot open snapshot field %d in %s\n", q, dir);
+            res = AC_FAILURE;
+            break;
+        }
+        for (int k = 0; k < g.nz && res == AC_SUCCESS; ++k)
+            for (int j = 0; j < g.ny; ++j) {
+                double* row = buf + NGHOST + (size_t)g.mx * ((j + NGHOST) +
+                                                            (size_t)g.my * (k + NGHOST));
+                if (fread(row, sizeof(double), g.nx, fp) != (size_t)g.nx) {
+                    res = AC_FAILURE;
+                    break;
+                }
+            }
+        /* the file must hold exactly the interior */
+        if (res == AC_SUCCESS && fgetc(fp) != EOF)
+            res = AC_FAILURE;
+        fclose(fp);
+        if (res != AC_SUCCESS)
+            break;
+        AcMesh m;
+        memset(&m, 0, sizeof(m));
+        m.info            = d->config;
+        m.vertex_buffer[q] = buf;
+        res = acDeviceLoadVertexBuffer(d, STREAM_DEFAULT, m, (VertexBufferHandle)q);
+        if (res == AC_SUCCESS && cudaStreamSynchronize(d->streams[STREAM_DEFAULT]) != cudaSuccess)
+            res = AC_FAILURE;
+    }
+    free(buf);
+    if (res != AC_SUCCESS)
+        return res;
+    /* the halos follow from the interior by the periodic fill */
+    const Volume m0 = {0, 0, 0};
+    const Volume m1 = {(size_t)g.mx, (size_t)g.my, (size_t)g.mz};
+    res = acDevicePeriodicBoundconds(d, STREAM_DEFAULT, m0, m1);
+    if (res == AC_SUCCESS)
+        res = acDeviceSynchronizeStream(d, STREAM_DEFAULT);
+    return res;
 }
 
 extern "C" void*

@@ -460,3 +460,98 @@ acHostMeshSolenoidalModes(AcMesh* mesh, const unsigned long long seed, const int
     free(ph);
     return AC_SUCCESS;
 }
+
+/* ---- snapshots in the reference's host format: src/utils/memory.cc:182-247 ----
+ * data-format.csv ("use_double, mx, my, mz" and one line of values) and one
+ * raw file <field name>-<id, 5 digits>.dat per field holding every cell
+ * (halos included, x fastest), in the current directory.  The format is kept
+ * so that files written by either code read in the other. */
+static const char kDataFormat[] = "data-format.csv";
+static const char* const kFieldNames[NUM_VTXBUF_HANDLES] = {
+    "VTXBUF_LNRHO", "VTXBUF_UUX", "VTXBUF_UUY", "VTXBUF_UUZ",
+    "VTXBUF_AX",    "VTXBUF_AY",  "VTXBUF_AZ",  "VTXBUF_ENTROPY"};
+
+static int
+grid_mm(const AcMeshInfo* in, int3* mm)
+{
+    AcMeshInfo info = *in;
+    if (acHostUpdateParams(&info) != AC_SUCCESS)
+        return 0;
+    *mm = info.int3_params[AC_mgrid];
+    return 1;
+}
+
+AcResult
+acHostMeshWriteToFile(const AcMesh mesh, const size_t id)
+{
+    int3 mm;
+    if (!grid_mm(&mesh.info, &mm))
+        return AC_FAILURE;
+    for (int q = 0; q < NUM_VTXBUF_HANDLES; ++q)
+        if (!mesh.vertex_buffer[q])
+            return AC_NOT_ALLOCATED;
+    FILE* header = fopen(kDataFormat, "w");
+    if (!header)
+        return AC_FAILURE;
+    fprintf(header, "use_double, mx, my, mz\n");
+    fprintf(header, "%d, %ld, %ld, %ld\n", (int)(sizeof(AcReal) == 8), (long)mm.x, (long)mm.y,
+            (long)mm.z);
+    if (fclose(header) != 0)
+        return AC_FAILURE;
+    const size_t count = (size_t)mm.x * (size_t)mm.y * (size_t)mm.z;
+    for (int q = 0; q < NUM_VTXBUF_HANDLES; ++q) {
+        char path[4096];
+        const int n = snprintf(path, sizeof(path), "%s-%.5lu.dat", kFieldNames[q],
+                               (unsigned long)id);
+        if (n < 0 || (size_t)n >= sizeof(path))
+            return AC_FAILURE;
+        FILE* fp = fopen(path, "wb");
+        if (!fp)
+            return AC_FAILURE;
+        const size_t written = fwrite(mesh.vertex_buffer[q], sizeof(AcReal), count, fp);
+        if (fclose(fp) != 0 || written != count)
+            return AC_FAILURE;
+    }
+    return AC_SUCCESS;
+}
+
+AcResult
+acHostMeshReadFromFile(const size_t id, AcMesh* mesh)
+{
+    if (!mesh)
+        return AC_FAILURE;
+    int3 mm;
+    if (!grid_mm(&mesh->info, &mm))
+        return AC_FAILURE;
+    FILE* header = fopen(kDataFormat, "r");
+    if (!header)
+        return AC_FAILURE;
+    char line[4096];
+    int use_double = -1, mx = -1, my = -1, mz = -1;
+    const int ok = fgets(line, sizeof(line), header) != NULL &&
+                   fscanf(header, "%d, %d, %d, %d", &use_double, &mx, &my, &mz) == 4;
+    fclose(header);
+    if (!ok || use_double != (int)(sizeof(AcReal) == 8) || mx != mm.x || my != mm.y ||
+        mz != mm.z) {
+        fprintf(stderr, "astaroth_b200: %s does not describe this mesh\n", kDataFormat);
+        return AC_FAILURE;
+    }
+    const size_t count = (size_t)mm.x * (size_t)mm.y * (size_t)mm.z;
+    for (int q = 0; q < NUM_VTXBUF_HANDLES; ++q) {
+        if (!mesh->vertex_buffer[q])
+            return AC_NOT_ALLOCATED;
+        char path[4096];
+        const int n = snprintf(path, sizeof(path), "%s-%.5lu.dat", kFieldNames[q],
+                               (unsigned long)id);
+        if (n < 0 || (size_t)n >= sizeof(path))
+            return AC_FAILURE;
+        FILE* fp = fopen(path, "rb");
+        if (!fp)
+            return AC_FAILURE;
+        const size_t got = fread(mesh->vertex_buffer[q], sizeof(AcReal), count, fp);
+        fclose(fp);
+        if (got != count)
+            return AC_FAILURE;
+    }
+    return AC_SUCCESS;
+}

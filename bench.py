@@ -65,9 +65,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32comp", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
-    ap.add_argument("--workload", default="step512", choices=["step512", "cfl1024"],
+    ap.add_argument("--workload", default="step512",
+                    choices=["step512", "cfl1024", "adjoint64"],
                     help="step512: the FP64 RK3 step (default line); cfl1024: 1024^3 "
-                         "FP32-compensated run with adaptive CFL timesteps")
+                         "FP32-compensated run with adaptive CFL timesteps; adjoint64: "
+                         "gradient of the final energy through 200 steps at 64^3")
     ap.add_argument("--accuracy-steps", type=int, default=100)
     return ap.parse_args()
 
@@ -279,7 +281,7 @@ def run_gpu(args):
     alg_bytes_step = BYTES_PER_CELL_STEP["fp64"] * cells
     peak, peak_kind = peaks()
     achieved = alg_bytes_step / (solve_step_ms * 1e-3) / 1e9
-    traffic = profile_traffic("solve_fp64_512.txt")
+    traffic = profile_traffic("solve_tiled_fp64_256.md")
 
     # ---- e2e through the C ABI with pinned host buffers
     e2e = None
@@ -340,6 +342,9 @@ def run_gpu(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "solve (3 launches per RK3 step)",
+                         "alg_bytes_per_launch": alg_bytes_step / 3,
+                         "traffic_source": "profiles/solve_tiled_fp64_256.md (ncu dram bytes at "
+                                           "256^3 scaled by the cell count to 512^3)",
                          "bytes_per_cell_step": BYTES_PER_CELL_STEP["fp64"],
                          "peak_source": peak_kind, "solve_ms_per_step": solve_step_ms,
                          "boundconds_ms_per_step": sum(bc_ms[-3:])},
@@ -628,10 +633,65 @@ def run_cfl1024(args):
     print(json.dumps(line), flush=True)
 
 
+def run_adjoint64(args):
+    """Gradient of J = E_kin + E_mag after 200 FP64 RK3 steps at 64^3 (dt = 1e-3,
+    seed 4, checkpoints every 20 steps) with respect to the initial fields and
+    nu, eta, through the torch.autograd wrapper over the C ABI: forward time,
+    backward time (recompute + reverse sweep) and their ratio, CUDA events on
+    torch's current stream with a device synchronisation on both sides."""
+    import torch
+    import astaroth_b200 as ab
+    from astaroth_b200 import autograd as AG
+
+    n, steps, every, dt = 64, 200, 20, 1e-3
+    torch.cuda.set_device(0)
+    info = ab.make_info(n, **ab.CONFIG_PARAMS)
+    f = torch.from_numpy(ab.seeded_mesh(info, 4)).cuda()
+    dev = ab.Device(info)
+    fwd, bwd = [], []
+    l0 = dev.launch_count()
+    for it in range(args.warmup + args.steps):
+        x0 = f.clone().requires_grad_(True)
+        nu = torch.tensor(5e-3, dtype=torch.float64, device="cuda", requires_grad=True)
+        eta = torch.tensor(5e-3, dtype=torch.float64, device="cuda", requires_grad=True)
+        torch.cuda.synchronize()
+        torch.cuda.reset_peak_memory_stats()
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        fN = AG.integrate(x0, nu, eta, dev, steps, dt, checkpoint_every=every)
+        J = AG.energy(fN, info)
+        e[1].record()
+        J.backward()
+        e[2].record()
+        torch.cuda.synchronize()
+        if it >= args.warmup:
+            fwd.append(e[0].elapsed_time(e[1]))
+            bwd.append(e[1].elapsed_time(e[2]))
+    launches = dev.launch_count() - l0
+    dev.destroy()
+    tf, tb = statistics.median(fwd), statistics.median(bwd)
+    line = {"metric": "adjoint cost: backward (recompute + reverse sweep) / forward time",
+            "value": tb / tf, "unit": "x", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seed 4, benchmark "
+            "distributions)",
+            "config": {"workload": f"{n}^3, {steps} RK3 steps, dt={dt}, checkpoints every "
+                                   f"{every} steps, J = E_kin + E_mag at the final time",
+                       "n": n},
+            "forward_ms": tf, "backward_ms": tb,
+            "forward_ms_per_step": tf / steps, "backward_ms_per_step": tb / steps,
+            "peak_torch_bytes": torch.cuda.max_memory_allocated(),
+            "gpu_launches": launches}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.workload == "cfl1024":
         run_cfl1024(args)
+        return
+    if args.workload == "adjoint64":
+        run_adjoint64(args)
         return
     if args.impl == "reference":
         run_reference(args)

@@ -10,6 +10,7 @@
  *   acHostMeshApplyPeriodicBounds  src/utils/memory.cc:76-149
  *   acHostReduceScal/Vec/VecScal   src/utils/modelreduce.cc:108-340
  *   acGetError                     src/utils/verification.cc:45-83
+ *   acHostMeshWriteToFile/ReadFromFile  src/utils/memory.cc:182-247 (snapshot format)
  * The two mesh helpers below stand in for src/core/astaroth.cc:324-335,425-431.
  */
 #include <stdlib.h>
@@ -155,4 +156,22 @@ ref_verify(double* const* model, double* const* candidate, const int nx, const i
                    AC_SUCCESS
                ? 0
                : 1;
+}
+
+/* The reference's snapshot writer and reader: data-format.csv and
+ * <field>-<id>.dat in the current directory.  Returns 0 on success. */
+extern "C" int
+ref_write_to_file(double* const* fields, const int nx, const int ny, const int nz,
+                  const unsigned long id)
+{
+    AcMesh mesh = make_mesh(fields, nx, ny, nz, NULL);
+    return acHostMeshWriteToFile(mesh, (size_t)id) == AC_SUCCESS ? 0 : 1;
+}
+
+extern "C" int
+ref_read_from_file(double* const* fields, const int nx, const int ny, const int nz,
+                   const unsigned long id)
+{
+    AcMesh mesh = make_mesh(fields, nx, ny, nz, NULL);
+    return acHostMeshReadFromFile((size_t)id, &mesh) == AC_SUCCESS ? 0 : 1;
 }

@@ -296,6 +296,8 @@ AcResult acHostMeshDestroy(AcMesh* mesh);
 /* Declarations of the reference functions compiled from the model files. */
 AcResult acHostMeshApplyPeriodicBounds(AcMesh* mesh);
 AcResult acHostIntegrateStep(AcMesh mesh, const AcReal dt);
+AcResult acHostMeshWriteToFile(const AcMesh mesh, const size_t id);
+AcResult acHostMeshReadFromFile(const size_t id, AcMesh* mesh);
 AcReal acHostReduceScal(const AcMesh mesh, const AcReduction reduction, const VertexBufferHandle a);
 AcReal acHostReduceVec(const AcMesh mesh, const AcReduction reduction, const VertexBufferHandle a,
                        const VertexBufferHandle b, const VertexBufferHandle c);
