@@ -1,6 +1,8 @@
 """Device snapshots (acDeviceWriteMeshToDisk / acDeviceReadMeshFromDisk) on
-the GPU: the files hold exactly the interior of the in-buffers, a restart from
-them continues bit for bit, and the halos come back as the periodic fill."""
+the GPU: the files hold exactly the interior of the in-buffers, the restored
+state is bit-identical with its halos as the periodic fill, and a restart
+continues bit for bit in FP64 (within FP32 rounding for FP32-compensated
+meshes, whose (hi, lo) pairs are re-split from the stored doubles)."""
 import numpy as np
 import pytest
 
@@ -42,7 +44,14 @@ def test_write_read_restart(tmp_path, precision, segmented):
         b.integrate_step(1e-3)
         b.synchronize()
         got = b.store_mesh()
-    assert np.array_equal(got[:, 3:-3, 3:-3, 3:-3], want[:, 3:-3, 3:-3, 3:-3])
+    if precision == 0:
+        assert np.array_equal(got[:, 3:-3, 3:-3, 3:-3], want[:, 3:-3, 3:-3, 3:-3])
+    else:
+        # The file holds hi + lo as a double.  Splitting it again gives the same
+        # pair except where lo was exactly half an ulp of hi (a rounding tie):
+        # the same value, but the stencils read hi, so the next step may differ
+        # at FP32 rounding level.
+        assert oracle.rel_linf(got, want).max() <= 1e-6
 
 
 def test_read_errors(tmp_path):
