@@ -40,9 +40,10 @@ class IntParam(enum.IntEnum):
     AC_precision = 0
     AC_additive_timestep = 1
     AC_debug_plain_kernel = 2
+    AC_upwind = 3
 
 
-NUM_INT_PARAMS = 3
+NUM_INT_PARAMS = 4
 
 
 class Int3Param(enum.IntEnum):

@@ -114,11 +114,15 @@ ac_make_stencil(const AcMeshInfo& info, StencilCoef* sc)
     const double e[3] = {270.0 / 720.0, -27.0 / 720.0, 2.0 / 720.0};
     const AcReal3 inv = info.real3_params[AC_inv_ds];
     const double iv[3] = {inv.x, inv.y, inv.z};
+    /* upwinding: (1/60) (-20 f0 + 15 s1 - 6 s2 + s3) / ds, modelsolver.cc:424-492 */
+    const double u[4] = {-20.0 / 60.0, 15.0 / 60.0, -6.0 / 60.0, 1.0 / 60.0};
     for (int a = 0; a < 3; ++a) {
         for (int k = 0; k < 3; ++k)
             sc->d1[a][k] = c[k] * iv[a];
-        for (int k = 0; k < 4; ++k)
+        for (int k = 0; k < 4; ++k) {
             sc->d2[a][k] = d[k] * iv[a] * iv[a];
+            sc->up[a][k] = u[k] * iv[a];
+        }
     }
     const int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2};
     for (int m = 0; m < 3; ++m)
@@ -143,6 +147,7 @@ ac_make_phys(const AcMeshInfo& info, PhysConst* pc)
     pc->lnrho0       = r[AC_lnrho0];
     pc->inv_exp_lnT0 = exp(-r[AC_lnT0]);
     pc->K            = r[AC_K_heatcond];
+    pc->upwind       = info.int_params[AC_upwind] != 0;
 }
 
 static bool
@@ -1049,6 +1054,12 @@ ensure_adjoint(const Device d)
         fprintf(stderr, "astaroth_b200: the adjoint needs an FP64 device (AC_precision = 0)\n");
         return AC_FAILURE;
     }
+    if (d->config.int_params[AC_upwind]) {
+        /* |u| in the upwinding terms has no derivative at u = 0; the reverse
+         * pass covers the equations without them */
+        fprintf(stderr, "astaroth_b200: the adjoint does not cover AC_upwind\n");
+        return AC_FAILURE;
+    }
     if (d->adj_lf)
         return AC_SUCCESS;
     const size_t fb = (size_t)d->geom.cells * sizeof(double);
@@ -1125,6 +1136,8 @@ acDeviceIntegrateSubstepAdjoint(const Device d, const Stream stream, const int s
                                 const Volume start, const Volume end, const AcReal dt)
 {
     if (!d || !stream_ok(stream) || step_number < 0 || step_number > 2 || !d->adj_lf)
+        return AC_FAILURE;
+    if (ensure_adjoint(d) != AC_SUCCESS)
         return AC_FAILURE;
     if (!is_whole_interior(d, start, end)) {
         fprintf(stderr, "astaroth_b200: acDeviceIntegrateSubstepAdjoint needs the whole interior\n");
@@ -1221,6 +1234,8 @@ acDeviceAdjointTapeBackward(const Device d, const Stream stream, const int steps
                             const AcReal dt)
 {
     if (!d || !stream_ok(stream) || steps < 1 || !d->adj_lf || d->adj_tape_states < 3 * steps)
+        return AC_FAILURE;
+    if (ensure_adjoint(d) != AC_SUCCESS)
         return AC_FAILURE;
     AC_CUDA_CHECK(cudaSetDevice(d->id));
     cudaStream_t st             = d->streams[stream];

@@ -519,6 +519,11 @@ acEnsembleCreate(const int device_id, const int n, const AcMeshInfo* configs, En
             destroy(e);
             return AC_FAILURE;
         }
+        if (info.int_params[AC_upwind]) {
+            fprintf(stderr, "astaroth_b200: ensemble members without AC_upwind only\n");
+            destroy(e);
+            return AC_FAILURE;
+        }
         e->precision = p;
         e->info.push_back(info);
         e->geom.push_back(ac_make_geom(info, p));

@@ -101,6 +101,7 @@ typedef struct {
 static const ParamName param_names[] = {
     {"AC_precision", 0, AC_precision},
     {"AC_additive_timestep", 0, AC_additive_timestep},
+    {"AC_upwind", 0, AC_upwind},
     {"AC_ngrid", 1, AC_ngrid},
     {"AC_nlocal", 1, AC_nlocal},
     {"AC_nu_visc", 2, AC_nu_visc},

@@ -55,6 +55,7 @@ struct PhysConst {
     double lnrho0;
     double inv_exp_lnT0;  /* exp(-lnT0) */
     double K;             /* K_heatcond */
+    int upwind;           /* AC_upwind: the LUPWD terms (selects the kernel variant) */
 };
 
 /* Stencil coefficients with the grid spacing folded in (6th order). */
@@ -63,6 +64,7 @@ struct StencilT {
     T d1[3][3];  /* [axis][k-1] = c_k / ds_axis, c = (3/4, -3/20, 1/60) */
     T d2[3][4];  /* [axis][k]   = d_k / ds_axis^2, d = (-49/18, 3/2, -3/20, 1/90) */
     T mix[3][3]; /* [xy,xz,yz][k-1] = e_k / (ds_a ds_b), e = (270,-27,2)/720 */
+    T up[3][4];  /* [axis][k] = u_k / ds_axis, u = (-20, 15, -6, 1)/60: upwinding */
 };
 typedef StencilT<double> StencilCoef;
 
@@ -76,8 +78,10 @@ stencil_cast(const StencilCoef& s)
             o.d1[a][k]  = (T)s.d1[a][k];
             o.mix[a][k] = (T)s.mix[a][k];
         }
-        for (int k = 0; k < 4; ++k)
+        for (int k = 0; k < 4; ++k) {
             o.d2[a][k] = (T)s.d2[a][k];
+            o.up[a][k] = (T)s.up[a][k];
+        }
     }
     return o;
 }

@@ -222,6 +222,21 @@ mag_rates(const ScalD<T>& Sg, const VecD<T>& A, const MagToHydro<T>& m, const Hy
     r[3]         = -(ux * Sg.g[0] + uy * Sg.g[1] + uz * Sg.g[2]) + heating + heat;
 }
 
+/* The upwinding terms (the reference's LUPWD option, mhdsolver.ac:336-338,
+ * 357-359; model src/utils/modelsolver.cc:776-779,837-841) added to the
+ * hydro rates: r[0] += |u| . upwd(lnrho), r[1 + c] += upwd(u_c) . |u|.
+ * up_l[a] and up_u[c][a] are the upwinding derivatives along axis a. */
+template <typename T>
+__device__ __forceinline__ void
+upwind_terms(const T up_l[3], const T up_u[3][3], const T u[3], T add[4])
+{
+    const T au[3] = {fabs(u[0]), fabs(u[1]), fabs(u[2])};
+    add[0]        = au[0] * up_l[0] + au[1] * up_l[1] + au[2] * up_l[2];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        add[1 + c] = up_u[c][0] * au[0] + up_u[c][1] * au[1] + up_u[c][2] * au[2];
+}
+
 /* rates[8] in field order (lnrho, ux, uy, uz, ax, ay, az, entropy). */
 template <typename T>
 __device__ __forceinline__ void

@@ -18,7 +18,7 @@ namespace {
 
 /* Every thread reaches the single cfl_commit at the end (it uses full-warp
  * shuffles and a block barrier), so there is no early return. */
-template <typename T, bool COMP>
+template <typename T, bool COMP, bool UPWD>
 __global__ void __launch_bounds__(128)
 solve_plain_kernel(const Geom g, const FieldsT<T> f, const StencilT<T> sc, const PhysConst pc,
                    const RkCoef rk, unsigned long long* cfl)
@@ -29,7 +29,7 @@ solve_plain_kernel(const Geom g, const FieldsT<T> f, const StencilT<T> sc, const
     const int k = blockIdx.z;
     T cm[3]     = {0, 0, 0};
     if (i < g.nx && j < g.ny && k < g.nz)
-        plain_cell<T, COMP>(g, PtrFieldsT<T>{f}, sc, pc, rk, cfl != nullptr, i, j, k, cm);
+        plain_cell<T, COMP, UPWD>(g, PtrFieldsT<T>{f}, sc, pc, rk, cfl != nullptr, i, j, k, cm);
     if (cfl)
         cfl_commit(cm, red, cfl);
 }
@@ -42,7 +42,12 @@ launch_plain(const Geom& g, const FieldsT<T>& f, const StencilCoef& sc, const Ph
 {
     const dim3 tpb(32, 4, 1);
     const dim3 bpg((g.nx + tpb.x - 1) / tpb.x, (g.ny + tpb.y - 1) / tpb.y, g.nz);
-    solve_plain_kernel<T, COMP><<<bpg, tpb, 0, stream>>>(g, f, stencil_cast<T>(sc), pc, rk, cfl);
+    if (pc.upwind)
+        solve_plain_kernel<T, COMP, true><<<bpg, tpb, 0, stream>>>(g, f, stencil_cast<T>(sc), pc,
+                                                                  rk, cfl);
+    else
+        solve_plain_kernel<T, COMP, false><<<bpg, tpb, 0, stream>>>(g, f, stencil_cast<T>(sc), pc,
+                                                                   rk, cfl);
     if (launches)
         ++*launches;
     return cudaGetLastError();

@@ -42,8 +42,9 @@ struct PtrFieldsT {
 };
 
 /* One cell of the plain kernel; adds the cell's CFL quantities to cm when cfl
- * is set.  F gives the field arrays (BlockFieldsT or PtrFieldsT). */
-template <typename T, bool COMP, typename F>
+ * is set.  F gives the field arrays (BlockFieldsT or PtrFieldsT); UPWD adds
+ * the upwinding terms (AC_upwind). */
+template <typename T, bool COMP, bool UPWD = false, typename F>
 static __device__ __forceinline__ void
 plain_cell(const Geom& g, const F& f, const StencilT<T>& sc, const PhysConst& pc,
            const RkCoef& rk, const bool cfl, const int i, const int j, const int k, T cm[3])
@@ -75,6 +76,21 @@ plain_cell(const Geom& g, const F& f, const StencilT<T>& sc, const PhysConst& pc
     const PhysT<T> p = phys_cast<T>(pc);
     T r[AC_NF];
     mhd_rates(L, S, U, A, p, r);
+    if constexpr (UPWD) {
+        T up_l[3], up_u[3][3], add[4];
+        const T* lf = f.in_p(VTXBUF_LNRHO) + idx;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            up_l[a] = der_up(lf, st[a], sc.up[a]);
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                up_u[c][a] = der_up(f.in_p(VTXBUF_UUX + c) + idx, st[a], sc.up[a]);
+        }
+        upwind_terms(up_l, up_u, U.v, add);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            r[q] += add[q];
+    }
 
     if (cfl) {
         const T Bx = A.g[2][1] - A.g[1][2], By = A.g[0][2] - A.g[2][0], Bz = A.g[1][0] - A.g[0][1];

@@ -169,6 +169,18 @@ d2_sides(const Taps<T>& t, const int q, const T* d)
     return r;
 }
 
+/* upwinding derivative along axis A: u_0 f + sum_k u_k (f[+k] + f[-k]) */
+template <int A, typename T>
+__device__ __forceinline__ T
+dup(const Taps<T>& t, const int q, const T* u)
+{
+    T r = u[0] * t(q, 0, 0, 0);
+    r   = fma(u[1], tap1<A>(t, q, 1) + tap1<A>(t, q, -1), r);
+    r   = fma(u[2], tap1<A>(t, q, 2) + tap1<A>(t, q, -2), r);
+    r   = fma(u[3], tap1<A>(t, q, 3) + tap1<A>(t, q, -3), r);
+    return r;
+}
+
 /* tap at +a along axis A and +b along axis B (A < B) */
 template <int A, int B, typename T>
 __device__ __forceinline__ T
@@ -230,7 +242,7 @@ vec_derivs(const Taps<T>& t, const int q0, const StencilT<T>& sc, VecD<T>& o)
     o.gd[2] = dmix<0, 2>(t, q0, sc.mix[1]) + dmix<1, 2>(t, q0 + 1, sc.mix[2]) + diag[2];
 }
 
-template <typename T, bool COMP>
+template <typename T, bool COMP, bool UPWD>
 __global__ void __launch_bounds__(2 * TX * TY, Tile<T>::MINB)
 solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const FieldsT<T> f,
                    const StencilT<T> sc, const PhysConst pc, const RkCoef rk, int* err,
@@ -326,11 +338,25 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
         HydroToMag<T> hx;
         MagToHydro<T> mx;
         Strain<T> st;
+        T upr[4] = {0, 0, 0, 0}; /* upwinding terms of the hydro rates (UPWD) */
         if (active) {
             if (group == 0) {
                 scal_derivs(t, VTXBUF_LNRHO, sc, sd);
                 vec_derivs(t, VTXBUF_UUX, sc, vd);
                 hydro_prepare(sd, t(VTXBUF_ENTROPY, 0, 0, 0), vd, p, hx, st);
+                if constexpr (UPWD) {
+                    const T up_l[3] = {dup<0>(t, VTXBUF_LNRHO, sc.up[0]),
+                                       dup<1>(t, VTXBUF_LNRHO, sc.up[1]),
+                                       dup<2>(t, VTXBUF_LNRHO, sc.up[2])};
+                    T up_u[3][3];
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) {
+                        up_u[c][0] = dup<0>(t, VTXBUF_UUX + c, sc.up[0]);
+                        up_u[c][1] = dup<1>(t, VTXBUF_UUX + c, sc.up[1]);
+                        up_u[c][2] = dup<2>(t, VTXBUF_UUX + c, sc.up[2]);
+                    }
+                    upwind_terms(up_l, up_u, vd.v, upr);
+                }
 #pragma unroll
                 for (int k = 0; k < AC_H2M_COUNT; ++k)
                     xh[k * NCELL + cell] = hx.a[k];
@@ -352,6 +378,11 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
                 for (int k = 0; k < AC_M2H_COUNT; ++k)
                     mx.a[k] = xm[k * NCELL + cell];
                 hydro_rates(sd, vd, st, hx, mx, p, r);
+                if constexpr (UPWD) {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        r[k] += upr[k];
+                }
                 val[0] = sd.v;
                 val[1] = vd.v[0];
                 val[2] = vd.v[1];
@@ -467,8 +498,12 @@ launch_tiled(const Geom& g, const void* tmap_in, const FieldsT<T>& f, const Sten
     const dim3 tpb(TX, 2 * TY, 1);
     const int zc = zchunk_for(g);
     const dim3 bpg((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + zc - 1) / zc);
-    solve_tiled_kernel<T, COMP><<<bpg, tpb, Layout<T>::SMEM_BYTES, stream>>>(
-        *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err, cfl, zc);
+    if (pc.upwind)
+        solve_tiled_kernel<T, COMP, true><<<bpg, tpb, Layout<T>::SMEM_BYTES, stream>>>(
+            *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err, cfl, zc);
+    else
+        solve_tiled_kernel<T, COMP, false><<<bpg, tpb, Layout<T>::SMEM_BYTES, stream>>>(
+            *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err, cfl, zc);
     if (launches)
         ++*launches;
     return cudaGetLastError();
@@ -500,11 +535,23 @@ ac_make_tensor_map(void* map_out, void* base, const Geom& g, const int precision
 cudaError_t
 ac_solve_tiled_init(const int precision)
 {
-    if (precision == 0)
-        return cudaFuncSetAttribute(solve_tiled_kernel<double, false>,
+    /* both variants (with and without the upwinding terms) */
+    if (precision == 0) {
+        const cudaError_t e = cudaFuncSetAttribute(solve_tiled_kernel<double, false, false>,
+                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)Layout<double>::SMEM_BYTES);
+        if (e != cudaSuccess)
+            return e;
+        return cudaFuncSetAttribute(solve_tiled_kernel<double, false, true>,
                                     cudaFuncAttributeMaxDynamicSharedMemorySize,
                                     (int)Layout<double>::SMEM_BYTES);
-    return cudaFuncSetAttribute(solve_tiled_kernel<float, true>,
+    }
+    const cudaError_t e = cudaFuncSetAttribute(solve_tiled_kernel<float, true, false>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)Layout<float>::SMEM_BYTES);
+    if (e != cudaSuccess)
+        return e;
+    return cudaFuncSetAttribute(solve_tiled_kernel<float, true, true>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)Layout<float>::SMEM_BYTES);
 }

@@ -42,6 +42,18 @@ der2_sides(const T* f, const long long s, const T* d)
     return r;
 }
 
+/* upwinding derivative: u_0 f + sum_k u_k (f[+ks] + f[-ks]), k = 1..3 */
+template <typename T>
+__device__ __forceinline__ T
+der_up(const T* f, const long long s, const T* u)
+{
+    T r = u[0] * ld(f);
+    r   = fma(u[1], ld(f + s) + ld(f - s), r);
+    r   = fma(u[2], ld(f + 2 * s) + ld(f - 2 * s), r);
+    r   = fma(u[3], ld(f + 3 * s) + ld(f - 3 * s), r);
+    return r;
+}
+
 /* sum_k e_k (f(+k,+k) + f(-k,-k) - f(+k,-k) - f(-k,+k)) along strides a, b */
 template <typename T>
 __device__ __forceinline__ T

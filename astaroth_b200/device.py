@@ -44,7 +44,9 @@ def make_info(n, precision: int = 0, **params) -> AcMeshInfo:
     _check(lib.acHostMeshInfoDefault(nx, ny, nz, C.byref(info)), "acHostMeshInfoDefault")
     info.int_params[IntParam.AC_precision] = precision
     for k, v in params.items():
-        if k == "ds":
+        if k == "upwind":
+            info.int_params[IntParam.AC_upwind] = int(v)
+        elif k == "ds":
             info.real3_params[Real3Param.AC_ds] = capi.Real3(*v)
         else:
             info.real_params[RealParam["AC_" + k]] = float(v)
@@ -60,7 +62,8 @@ def info_to_dict(info: AcMeshInfo) -> dict:
                 cs_sound=r[RealParam.AC_cs_sound], gamma=r[RealParam.AC_gamma],
                 cp_sound=r[RealParam.AC_cp_sound], lnrho0=r[RealParam.AC_lnrho0],
                 lnT0=r[RealParam.AC_lnT0], mu0=r[RealParam.AC_mu0], zeta=r[RealParam.AC_zeta],
-                K_heatcond=r[RealParam.AC_K_heatcond])
+                K_heatcond=r[RealParam.AC_K_heatcond],
+                upwind=info.int_params[IntParam.AC_upwind])
 
 
 def dims(info: AcMeshInfo):

@@ -66,6 +66,16 @@ d2(const R p[7], const R inv_ds)
     return s * inv_ds * inv_ds;
 }
 
+/* Upwinding stencil (a scaled 6th derivative), der6x_upwd of
+ * modelsolver.cc:424-492 with the same order of operations. */
+static inline R
+d6up(const R p[7], const R inv_ds)
+{
+    return (R)(1.0 / 60.0) * inv_ds *
+           (-(R)(20.0) * p[3] + (R)(15.0) * (p[4] + p[2]) - (R)(6.0) * (p[5] + p[1]) + p[6] +
+            p[0]);
+}
+
 /* Diagonal cross stencil: a runs along (+,+), b along (+,-). */
 static inline R
 dmix(const R a[7], const R b[7], const R inv_a, const R inv_b)
@@ -85,6 +95,7 @@ typedef struct {
     R v;
     V3 g;
     R h[3][3];
+    V3 up; /* upwinding derivatives (modelsolver.cc:501-506), LUPWD only */
 } Deriv;
 
 static void
@@ -104,6 +115,9 @@ derivs(const double* f, const Dims* d, const int i, const int j, const int k, co
     out->h[0][0] = d2(px, inv[0]);
     out->h[1][1] = d2(py, inv[1]);
     out->h[2][2] = d2(pz, inv[2]);
+    out->up.x    = d6up(px, inv[0]);
+    out->up.y    = d6up(py, inv[1]);
+    out->up.z    = d6up(pz, inv[2]);
     if (need_mixed) {
         R a[7], b[7];
         for (int o = 0; o < 7; ++o) {
@@ -252,9 +266,14 @@ rates(const double* const* f, const Dims* d, const int i, const int j, const int
             cp = p->cp_sound, lnrho0 = p->lnrho0, lnT0 = p->lnT0, mu0 = p->mu0,
             zeta = p->zeta, K = p->K_heatcond;
     const V3 u = vecvalue(uu);
+    /* |u| (vecvalue_abs, modelsolver.cc:579-586) for the LUPWD terms */
+    const V3 au = {fabsl(u.x), fabsl(u.y), fabsl(u.z)};
 
-    /* continuity */
-    out[LNRHO] = -dot3(u, lnrho.g) - divergence(uu);
+    /* continuity; with LUPWD + dot(|u|, upwd(lnrho)) before the divergence */
+    if (p->upwind)
+        out[LNRHO] = -dot3(u, lnrho.g) + dot3(au, lnrho.up) - divergence(uu);
+    else
+        out[LNRHO] = -dot3(u, lnrho.g) - divergence(uu);
 
     /* induction (gauge without grad div A) */
     {
@@ -280,6 +299,10 @@ rates(const double* const* f, const Dims* d, const int i, const int j, const int
         const V3 visc    = add3(add3(lapvec(uu), scale3((R)(1. / 3.), graddiv(uu))),
                                 scale3((R)(2.), SgL));
         V3 m = sub3(neg3(gradmul(uu, u)), scale3(cs2, pgrad));
+        if (p->upwind) { /* + mul(gradients_upwd(uu), |u|), modelsolver.cc:837-841 */
+            const V3 up = {dot3(uu[0].up, au), dot3(uu[1].up, au), dot3(uu[2].up, au)};
+            m           = add3(m, up);
+        }
         m    = add3(m, scale3(inv_rho, cross3(jj, B)));
         m    = add3(m, scale3(nu, visc));
         m    = add3(m, scale3(zeta, graddiv(uu)));

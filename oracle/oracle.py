@@ -4,6 +4,7 @@
 * ``reference`` -- _ref/libastaroth_ref.so, the reference's own host model files
                    (src/utils/{modelsolver,memory,modelreduce,verification}.cc)
                    compiled unchanged against oracle/shim (oracle/Makefile).
+* ``reference_upwd`` -- the same built with LUPWD=1 (the upwinding terms).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
 module, as the checker; the product library never loads it.  Meshes are
@@ -21,6 +22,8 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 PORT_LIB = HERE / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libastaroth_ref.so"
+REF_UPWD_LIB = HERE / "_ref" / "libastaroth_ref_upwd.so"
+_PATHS = {"port": PORT_LIB, "reference": REF_LIB, "reference_upwd": REF_UPWD_LIB}
 REF_SRC = Path(os.environ.get("AC_REFERENCE", "/root/reference"))
 
 RTYPE_NAMES = ["RTYPE_MAX", "RTYPE_MIN", "RTYPE_SUM", "RTYPE_RMS", "RTYPE_RMS_EXP",
@@ -31,7 +34,7 @@ class OracleParams(C.Structure):
     _fields_ = [("ds", C.c_double * 3), ("nu_visc", C.c_double), ("eta", C.c_double),
                 ("cs_sound", C.c_double), ("gamma", C.c_double), ("cp_sound", C.c_double),
                 ("lnrho0", C.c_double), ("lnT0", C.c_double), ("mu0", C.c_double),
-                ("zeta", C.c_double), ("K_heatcond", C.c_double)]
+                ("zeta", C.c_double), ("K_heatcond", C.c_double), ("upwind", C.c_int)]
 
 
 def make_params(p: dict) -> OracleParams:
@@ -40,6 +43,7 @@ def make_params(p: dict) -> OracleParams:
     for k in ("nu_visc", "eta", "cs_sound", "gamma", "cp_sound", "lnrho0", "lnT0", "mu0", "zeta",
               "K_heatcond"):
         setattr(o, k, float(p[k]))
+    o.upwind = int(p.get("upwind", 0))
     return o
 
 
@@ -52,13 +56,13 @@ _libs: dict[str, C.CDLL] = {}
 
 
 def available(kind: str) -> bool:
-    return (PORT_LIB if kind == "port" else REF_LIB).exists()
+    return _PATHS[kind].exists()
 
 
 def lib(kind: str = "port") -> C.CDLL:
     if kind in _libs:
         return _libs[kind]
-    path = PORT_LIB if kind == "port" else REF_LIB
+    path = _PATHS[kind]
     if not path.exists():
         raise RuntimeError(f"oracle library {path} is missing (run `make -C oracle`)")
     L = C.CDLL(str(path))

@@ -18,4 +18,6 @@ typedef struct {
     double mu0;
     double zeta;
     double K_heatcond;
+    int upwind; /* 1: the LUPWD terms (restatement only; the reference model
+                   takes LUPWD at compile time, libastaroth_ref_upwd.so) */
 } OracleParams;

@@ -37,7 +37,9 @@ using std::isnan;
 #define LMAGNETIC (1)
 #define LENTROPY (1)
 #define LTEMPERATURE (0)
+#ifndef LUPWD /* the upwinding variant of the model is built with -DLUPWD=1 */
 #define LUPWD (0)
+#endif
 #define LBFIELD (0)
 #define LFORCING (0)
 #define LSHOCK (0)

@@ -88,6 +88,24 @@ def test_port_matches_reference_bitexact(n, seed):
     assert np.array_equal(c, d)
 
 
+@pytest.mark.skipif(not oracle.available("reference_upwd"),
+                    reason="reference model with LUPWD=1 not built")
+@pytest.mark.parametrize("n,seed,amp", [(16, 41, 1e-3), ((14, 9, 7), 42, 5e-2)])
+def test_port_upwinding_matches_reference_bitexact(n, seed, amp):
+    """The LUPWD terms (modelsolver.cc:424-506,776-779,837-841) in the
+    restatement equal the reference model built with LUPWD=1, bit for bit,
+    and change the result (they are not a no-op)."""
+    info = make_info(n, **CONFIG_PARAMS)
+    p = dict(info_to_dict(info), upwind=1)
+    f = seeded_mesh(info, seed, amp_scalar=amp, sigma_uu=amp, sigma_aa=amp / 10)
+    a, b, c = f.copy(), f.copy(), f.copy()
+    oracle.integrate(a, p, 1e-3, 2, "port")
+    oracle.integrate(b, p, 1e-3, 2, "reference_upwd")
+    oracle.integrate(c, dict(p, upwind=0), 1e-3, 2, "port")
+    assert np.array_equal(a, b)
+    assert not np.array_equal(a, c)
+
+
 @needs_ref
 def test_port_matches_reference_other_params():
     """Non-default physics (larger amplitudes, other gamma/cp) stay bit-exact."""
