@@ -41,9 +41,10 @@ class IntParam(enum.IntEnum):
     AC_additive_timestep = 1
     AC_debug_plain_kernel = 2
     AC_upwind = 3
+    AC_lforcing = 4
 
 
-NUM_INT_PARAMS = 4
+NUM_INT_PARAMS = 5
 
 
 class Int3Param(enum.IntEnum):
@@ -77,9 +78,25 @@ class RealParam(enum.IntEnum):
     AC_current_time = 13
     AC_cs2_sound = 14
     AC_dsmin = 15
+    AC_forcing_magnitude = 16
+    AC_forcing_phase = 17
+    AC_k_forcex = 18
+    AC_k_forcey = 19
+    AC_k_forcez = 20
+    AC_ff_hel_rex = 21
+    AC_ff_hel_rey = 22
+    AC_ff_hel_rez = 23
+    AC_ff_hel_imx = 24
+    AC_ff_hel_imy = 25
+    AC_ff_hel_imz = 26
+    AC_kaver = 27
+    AC_switch_forcing = 28
+    AC_relhel = 29
+    AC_kmin = 30
+    AC_kmax = 31
 
 
-NUM_REAL_PARAMS = 16
+NUM_REAL_PARAMS = 32
 
 
 class Real3Param(enum.IntEnum):
@@ -242,6 +259,9 @@ SIGNATURES = {
     "acDeviceStoreAdjoint": (C.c_int, [Device_p, C.c_int, C.POINTER(C.c_void_p)]),
     "acDeviceGetParamAdjoints": (C.c_int, [Device_p, C.POINTER(C.c_double),
                                            C.POINTER(C.c_double)]),
+    "acHostForcingParams": (C.c_int, [Real3, C.c_double, C.c_double, C.POINTER(AcMeshInfo)]),
+    "acHostGenerateForcingParams": (C.c_int, [C.c_ulonglong, C.c_ulonglong,
+                                              C.POINTER(AcMeshInfo)]),
     "acHostMeshWriteToFile": (C.c_int, [AcMesh, C.c_size_t]),
     "acHostMeshReadFromFile": (C.c_int, [C.c_size_t, C.POINTER(AcMesh)]),
     "acDeviceWriteMeshToDisk": (C.c_int, [Device_p, C.c_char_p, C.c_char_p, C.c_int]),

@@ -148,6 +148,39 @@ ac_make_phys(const AcMeshInfo& info, PhysConst* pc)
     pc->inv_exp_lnT0 = exp(-r[AC_lnT0]);
     pc->K            = r[AC_K_heatcond];
     pc->upwind       = info.int_params[AC_upwind] != 0;
+    pc->forcing      = 0;
+    for (int a = 0; a < 3; ++a)
+        pc->f_k[a] = pc->f_re[a] = pc->f_im[a] = 0.0;
+    pc->f_cos_phase = 1.0;
+    pc->f_sin_phase = 0.0;
+    pc->f_scale     = 0.0;
+}
+
+/* The forcing of a substep-2 launch (mhdsolver.ac:531-541): active when
+ * AC_lforcing is set and AC_current_time > AC_switch_forcing. */
+static void
+forcing_for_launch(const AcMeshInfo& info, const double dt, PhysConst* pc)
+{
+    const double* r = info.real_params;
+    if (!info.int_params[AC_lforcing] || !(r[AC_current_time] > r[AC_switch_forcing]))
+        return;
+    const double two_pi = 6.283185307179586476925286766559;
+    const int3 ng       = info.int3_params[AC_ngrid];
+    const double k[3]   = {r[AC_k_forcex], r[AC_k_forcey], r[AC_k_forcez]};
+    const int n[3]      = {ng.x, ng.y, ng.z};
+    const double fre[3] = {r[AC_ff_hel_rex], r[AC_ff_hel_rey], r[AC_ff_hel_rez]};
+    const double fim[3] = {r[AC_ff_hel_imx], r[AC_ff_hel_imy], r[AC_ff_hel_imz]};
+    for (int a = 0; a < 3; ++a) {
+        pc->f_k[a]  = k[a] * two_pi / n[a];
+        pc->f_re[a] = fre[a];
+        pc->f_im[a] = fim[a];
+    }
+    pc->f_cos_phase = cos(r[AC_forcing_phase]);
+    pc->f_sin_phase = sin(r[AC_forcing_phase]);
+    /* N = cs magnitude sqrt(kaver cs); the force is sqrt(dt) N f */
+    const double cs = sqrt(r[AC_cs_sound] * r[AC_cs_sound]);
+    pc->f_scale     = sqrt(dt) * cs * r[AC_forcing_magnitude] * sqrt(r[AC_kaver] * cs);
+    pc->forcing     = 1;
 }
 
 static bool
@@ -647,6 +680,8 @@ launch_substep(Device d, cudaStream_t st, const int step, const double dt,
     PhysConst pc;
     ac_make_stencil(d->config, &sc);
     ac_make_phys(d->config, &pc);
+    if (step == 2)
+        forcing_for_launch(d->config, dt, &pc);
     const RkCoef rk = ac_rk_coef(step, dt);
     const int blk   = in_block_index(d);
     const bool tiled = d->solve_variant == 1 && d->tmap_ok && blk >= 0;

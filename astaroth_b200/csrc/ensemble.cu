@@ -519,8 +519,9 @@ acEnsembleCreate(const int device_id, const int n, const AcMeshInfo* configs, En
             destroy(e);
             return AC_FAILURE;
         }
-        if (info.int_params[AC_upwind]) {
-            fprintf(stderr, "astaroth_b200: ensemble members without AC_upwind only\n");
+        if (info.int_params[AC_upwind] || info.int_params[AC_lforcing]) {
+            fprintf(stderr, "astaroth_b200: ensemble members without AC_upwind and "
+                            "AC_lforcing only\n");
             destroy(e);
             return AC_FAILURE;
         }

@@ -87,6 +87,12 @@ acHostMeshInfoDefault(const int nx, const int ny, const int nz, AcMeshInfo* info
     info->real_params[AC_K_heatcond] = 1e-3;
     info->real_params[AC_cdt]       = 0.4;
     info->real_params[AC_cdtv]      = 0.3;
+    /* forcing: config/astaroth.conf:58-61 */
+    info->real_params[AC_relhel]            = 0.0;
+    info->real_params[AC_forcing_magnitude] = 1e-5;
+    info->real_params[AC_kmin]              = 0.8;
+    info->real_params[AC_kmax]              = 1.2;
+    info->real_params[AC_switch_forcing]    = 0.0;
     return acHostUpdateParams(info);
 }
 
@@ -102,6 +108,7 @@ static const ParamName param_names[] = {
     {"AC_precision", 0, AC_precision},
     {"AC_additive_timestep", 0, AC_additive_timestep},
     {"AC_upwind", 0, AC_upwind},
+    {"AC_lforcing", 0, AC_lforcing},
     {"AC_ngrid", 1, AC_ngrid},
     {"AC_nlocal", 1, AC_nlocal},
     {"AC_nu_visc", 2, AC_nu_visc},
@@ -117,6 +124,11 @@ static const ParamName param_names[] = {
     {"AC_cdt", 2, AC_cdt},
     {"AC_cdtv", 2, AC_cdtv},
     {"AC_chi", 2, AC_chi},
+    {"AC_relhel", 2, AC_relhel},
+    {"AC_forcing_magnitude", 2, AC_forcing_magnitude},
+    {"AC_kmin", 2, AC_kmin},
+    {"AC_kmax", 2, AC_kmax},
+    {"AC_switch_forcing", 2, AC_switch_forcing},
     {"AC_ds", 3, AC_ds},
 };
 
@@ -556,3 +568,111 @@ acHostMeshReadFromFile(const size_t id, AcMesh* mesh)
     }
     return AC_SUCCESS;
 }
+
+/* ---- forcing parameters: src/utils/astaroth_forcing.cc:84-256 ----
+ * The reference draws a wave vector from the integer shell kmin <= |k| <= kmax,
+ * the angle phi of the helical basis vector and the phase with its own random
+ * generator; acHostForcingParams takes those three draws as arguments and
+ * computes the rest as the reference does.  acHostGenerateForcingParams makes
+ * the draws from a counter-based generator (splitmix64 of seed and step), so a
+ * run is reproducible; its draws differ from the reference's generator. */
+static AcReal3
+v3(const double x, const double y, const double z)
+{
+    const AcReal3 r = {x, y, z};
+    return r;
+}
+
+static AcReal3
+cross3(const AcReal3 a, const AcReal3 b)
+{
+    return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+
+static AcReal3
+normalized3(const AcReal3 a)
+{
+    const double n = sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
+    return v3(a.x / n, a.y / n, a.z / n);
+}
+
+AcResult
+acHostForcingParams(const AcReal3 k_force, const AcReal phi, const AcReal phase, AcMeshInfo* info)
+{
+    if (!info)
+        return AC_FAILURE;
+    const double kk = k_force.x * k_force.x + k_force.y * k_force.y + k_force.z * k_force.z;
+    if (!(kk > 0.0))
+        return AC_FAILURE;
+    const double relhel = info->real_params[AC_relhel];
+    /* e: a unit vector perpendicular to k, rotated by phi about k
+     * (helical_forcing_e_generator, astaroth_forcing.cc:137-155) */
+    AcReal3 e = (k_force.y == 0.0 && k_force.z == 0.0) ? v3(0, 1, 0) : v3(1, 0, 0);
+    const AcReal3 kxe   = normalized3(cross3(k_force, e));
+    const AcReal3 kxkxe = normalized3(cross3(k_force, kxe));
+    e = v3(cos(phi) * kxe.x + sin(phi) * kxkxe.x, cos(phi) * kxe.y + sin(phi) * kxkxe.y,
+           cos(phi) * kxe.z + sin(phi) * kxkxe.z);
+    /* helical_forcing_special_vector, astaroth_forcing.cc:158-216 (Pencil Code
+     * forcing_hel_both): f_im = |k| (k x e) / D, f_re = relhel k x (k x e) / D */
+    const AcReal3 kdote = v3(k_force.x * e.x, k_force.y * e.y, k_force.z * e.z);
+    const AcReal3 ke    = cross3(k_force, e);
+    const AcReal3 kke   = cross3(k_force, ke);
+    const double kabs   = sqrt(kk);
+    const double den    = sqrt(1.0 + relhel * relhel) * kabs *
+                       sqrt(kabs * kabs -
+                            (kdote.x * kdote.x + kdote.y * kdote.y + kdote.z * kdote.z));
+    double* r                = info->real_params;
+    r[AC_ff_hel_imx]         = kabs * ke.x / den;
+    r[AC_ff_hel_imy]         = kabs * ke.y / den;
+    r[AC_ff_hel_imz]         = kabs * ke.z / den;
+    r[AC_ff_hel_rex]         = relhel * kke.x / den;
+    r[AC_ff_hel_rey]         = relhel * kke.y / den;
+    r[AC_ff_hel_rez]         = relhel * kke.z / den;
+    r[AC_k_forcex]           = k_force.x;
+    r[AC_k_forcey]           = k_force.y;
+    r[AC_k_forcez]           = k_force.z;
+    r[AC_forcing_phase]      = phase;
+    r[AC_kaver]              = (r[AC_kmax] - r[AC_kmin]) / 2.0;
+    return AC_SUCCESS;
+}
+
+AcResult
+acHostGenerateForcingParams(const unsigned long long seed, const unsigned long long step,
+                            AcMeshInfo* info)
+{
+    if (!info)
+        return AC_FAILURE;
+    const double kmin = info->real_params[AC_kmin], kmax = info->real_params[AC_kmax];
+    /* the integer shell of helical_forcing_k_generator, astaroth_forcing.cc:84-133 */
+    const int min_int = (int)ceil(kmin), max_int = (int)floor(kmax);
+    const double min2 = kmin * kmin, max2 = kmax * kmax;
+    const int min2i = min_int * min_int, max2i = max_int * max_int;
+    long count = 0;
+    for (int pass = 0; pass < 2; ++pass) {
+        long pick = -1, n = 0;
+        if (pass == 1) {
+            if (count == 0)
+                return AC_FAILURE;
+            const uint64_t c = splitmix64((uint64_t)seed * 0x9E3779B97F4A7C15ull + 3ull * step);
+            pick             = (long)(c % (uint64_t)count);
+        }
+        for (int x = -max_int; x <= max_int; ++x)
+            for (int y = -max_int; y <= max_int; ++y)
+                for (int z = -max_int; z <= max_int; ++z) {
+                    const int d2 = x * x + y * y + z * z;
+                    if ((min2 <= d2 || min2i == d2) && (max2 >= d2 || max2i == d2)) {
+                        if (pass == 1 && n == pick) {
+                            const double two_pi = 6.283185307179586476925286766559;
+                            const uint64_t b = (uint64_t)seed * 0x9E3779B97F4A7C15ull + 3ull * step;
+                            const double phi   = two_pi * u01(splitmix64(b + 1));
+                            const double phase = two_pi * u01(splitmix64(b + 2));
+                            return acHostForcingParams(v3(x, y, z), phi, phase, info);
+                        }
+                        ++n;
+                    }
+                }
+        count = n;
+    }
+    return AC_FAILURE;
+}
+

@@ -56,6 +56,14 @@ struct PhysConst {
     double inv_exp_lnT0;  /* exp(-lnT0) */
     double K;             /* K_heatcond */
     int upwind;           /* AC_upwind: the LUPWD terms (selects the kernel variant) */
+    /* helical forcing of this launch (substep 2 only; forcing = 0 otherwise):
+     * u += scale (re cos(a + phase) - im sin(a + phase)), a = sum_d f_k[d] idx_d
+     * with idx the interior cell index (mhdsolver.ac:286-331) */
+    int forcing;
+    double f_k[3];        /* k_force[d] 2 pi / ngrid[d] */
+    double f_re[3], f_im[3];
+    double f_cos_phase, f_sin_phase;
+    double f_scale;       /* sqrt(dt) cs magnitude sqrt(kaver cs) */
 };
 
 /* Stencil coefficients with the grid spacing folded in (6th order). */

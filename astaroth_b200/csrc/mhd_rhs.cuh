@@ -237,6 +237,36 @@ upwind_terms(const T up_l[3], const T up_u[3][3], const T u[3], T add[4])
         add[1 + c] = up_u[c][0] * au[0] + up_u[c][1] * au[1] + up_u[c][2] * au[2];
 }
 
+/* Helical forcing added to u in substep 2 at interior cell (i, j, k): the
+ * reference's forcing()/helical_forcing() (mhdsolver.ac:286-331; model
+ * src/utils/modelsolver.cc:1003-1076), with the phase angle k . (2 pi x / L)
+ * and scale sqrt(dt) cs magnitude sqrt(kaver cs) precomputed on the host. */
+template <typename T>
+__device__ __forceinline__ void
+forcing_at(const PhysConst& pc, const int i, const int j, const int k, T f[3])
+{
+    const double a = pc.f_k[0] * i + pc.f_k[1] * j + pc.f_k[2] * k;
+    double sa, ca;
+    sincos(a, &sa, &ca);
+    const double re = ca * pc.f_cos_phase - sa * pc.f_sin_phase;
+    const double im = ca * pc.f_sin_phase + sa * pc.f_cos_phase;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        f[c] = (T)(pc.f_scale * (pc.f_re[c] * re - pc.f_im[c] * im));
+}
+
+/* (h, l) += v for a compensated FP32 pair, renormalised (two-sum) */
+__device__ __forceinline__ void
+comp_add(float& h, float& l, const float v)
+{
+    const float s  = __fadd_rn(h, v);
+    const float bb = __fsub_rn(s, h);
+    const float e  = __fadd_rn(__fsub_rn(h, __fsub_rn(s, bb)), __fsub_rn(v, bb));
+    const float l2 = __fadd_rn(l, e);
+    h              = __fadd_rn(s, l2);
+    l              = __fsub_rn(l2, __fsub_rn(h, s));
+}
+
 /* rates[8] in field order (lnrho, ux, uy, uz, ax, ay, az, entropy). */
 template <typename T>
 __device__ __forceinline__ void

@@ -15,6 +15,7 @@
  * Layout: one array per field, x fastest, idx = i + mx*(j + my*k), with
  * mx = nx + 6 etc. and the interior at [3, n+3) on every axis.
  */
+#define _GNU_SOURCE /* M_PIl, as the reference model uses (modelsolver.cc:83) */
 #include <math.h>
 #include <stddef.h>
 #include <stdlib.h>
@@ -335,6 +336,43 @@ rates(const double* const* f, const Dims* d, const int i, const int j, const int
 }
 
 /* ---------------------------------------------------------------------------
+ * Helical forcing added to u in substep 2: forcing() and helical_forcing() of
+ * modelsolver.cc:1003-1076, applied as in :1162-1168, with the same order of
+ * operations in long double.  The scale is cs * magnitude * sqrt(kaver cs) as
+ * in the device code (mhdsolver.ac:318-319); the host model leaves the
+ * magnitude out, so the two agree bit for bit at magnitude 1.
+ * ------------------------------------------------------------------------- */
+static void
+forcing_vec(const OracleParams* p, const Dims* d, const int i, const int j, const int k,
+            const R dt, R out[3])
+{
+    const R ds[3] = {(R)p->ds[0], (R)p->ds[1], (R)p->ds[2]};
+    const int n[3] = {d->nx, d->ny, d->nz};
+    R xx[3]        = {(R)(i - HALO) * ds[0], (R)(j - HALO) * ds[1], (R)(k - HALO) * ds[2]};
+    for (int a = 0; a < 3; ++a)
+        xx[a] = xx[a] * ((R)2.0 * M_PIl / (ds[a] * n[a]));
+    const R phi     = (R)p->f_phase;
+    const R cos_phi = cosl(phi);
+    const R sin_phi = sinl(phi);
+    const R kx      = (R)p->f_k[0] * xx[0] + (R)p->f_k[1] * xx[1] + (R)p->f_k[2] * xx[2];
+    const R ckx     = cosl(kx);
+    const R skx     = sinl(kx);
+    const R re      = ckx * cos_phi - skx * sin_phi;
+    const R im      = ckx * sin_phi + skx * cos_phi;
+    const R cs2     = (R)(p->cs_sound * p->cs_sound); /* AC_cs2_sound, a double param */
+    const R cs      = sqrtl(cs2);
+    const R NN      = cs * (R)p->f_magnitude * sqrtl((R)p->f_kaver * cs);
+    int ok          = 1;
+    for (int a = 0; a < 3; ++a) {
+        const R f = (R)p->f_re[a] * re - (R)p->f_im[a] * im;
+        out[a]    = sqrtl(dt) * NN * f;
+        ok        = ok && !isnan(out[a]) && !isinf(out[a]);
+    }
+    if (!ok)
+        out[0] = out[1] = out[2] = 0;
+}
+
+/* ---------------------------------------------------------------------------
  * Periodic halo fill: src/utils/memory.cc:76-149 (every field communicated).
  * ------------------------------------------------------------------------- */
 static void
@@ -409,6 +447,12 @@ oracle_integrate(double* const* f, const int nx, const int ny, const int nz,
                         const size_t idx = at(&d, i, j, k);
                         for (int q = 0; q < NFIELDS; ++q)
                             f[q][idx] += (double)(beta[s] * (R)w[q][idx]);
+                        if (s == 2 && p->forcing) {
+                            R fu[3];
+                            forcing_vec(p, &d, i, j, k, (R)dt, fu);
+                            for (int c = 0; c < 3; ++c)
+                                f[UUX + c][idx] = (double)((R)f[UUX + c][idx] + fu[c]);
+                        }
                     }
         }
     }

@@ -5,6 +5,7 @@
                    (src/utils/{modelsolver,memory,modelreduce,verification}.cc)
                    compiled unchanged against oracle/shim (oracle/Makefile).
 * ``reference_upwd`` -- the same built with LUPWD=1 (the upwinding terms).
+* ``reference_forcing`` -- the same built with LFORCING=1 (helical forcing).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
 module, as the checker; the product library never loads it.  Meshes are
@@ -23,7 +24,9 @@ HERE = Path(__file__).resolve().parent
 PORT_LIB = HERE / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libastaroth_ref.so"
 REF_UPWD_LIB = HERE / "_ref" / "libastaroth_ref_upwd.so"
-_PATHS = {"port": PORT_LIB, "reference": REF_LIB, "reference_upwd": REF_UPWD_LIB}
+REF_FORCING_LIB = HERE / "_ref" / "libastaroth_ref_forcing.so"
+_PATHS = {"port": PORT_LIB, "reference": REF_LIB, "reference_upwd": REF_UPWD_LIB,
+          "reference_forcing": REF_FORCING_LIB}
 REF_SRC = Path(os.environ.get("AC_REFERENCE", "/root/reference"))
 
 RTYPE_NAMES = ["RTYPE_MAX", "RTYPE_MIN", "RTYPE_SUM", "RTYPE_RMS", "RTYPE_RMS_EXP",
@@ -34,7 +37,10 @@ class OracleParams(C.Structure):
     _fields_ = [("ds", C.c_double * 3), ("nu_visc", C.c_double), ("eta", C.c_double),
                 ("cs_sound", C.c_double), ("gamma", C.c_double), ("cp_sound", C.c_double),
                 ("lnrho0", C.c_double), ("lnT0", C.c_double), ("mu0", C.c_double),
-                ("zeta", C.c_double), ("K_heatcond", C.c_double), ("upwind", C.c_int)]
+                ("zeta", C.c_double), ("K_heatcond", C.c_double), ("upwind", C.c_int),
+                ("forcing", C.c_int), ("f_magnitude", C.c_double), ("f_phase", C.c_double),
+                ("f_kaver", C.c_double), ("f_k", C.c_double * 3), ("f_re", C.c_double * 3),
+                ("f_im", C.c_double * 3)]
 
 
 def make_params(p: dict) -> OracleParams:
@@ -44,6 +50,14 @@ def make_params(p: dict) -> OracleParams:
               "K_heatcond"):
         setattr(o, k, float(p[k]))
     o.upwind = int(p.get("upwind", 0))
+    o.forcing = int(p.get("forcing", 0))
+    if o.forcing:
+        o.f_magnitude = float(p["forcing_magnitude"])
+        o.f_phase = float(p["forcing_phase"])
+        o.f_kaver = float(p["kaver"])
+        o.f_k[:] = list(p["k_force"])
+        o.f_re[:] = list(p["ff_hel_re"])
+        o.f_im[:] = list(p["ff_hel_im"])
     return o
 
 

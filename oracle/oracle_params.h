@@ -20,4 +20,9 @@ typedef struct {
     double K_heatcond;
     int upwind; /* 1: the LUPWD terms (restatement only; the reference model
                    takes LUPWD at compile time, libastaroth_ref_upwd.so) */
+    /* helical forcing in substep 2 (restatement: when forcing != 0; the
+     * reference model built with LFORCING=1 always applies it) */
+    int forcing;
+    double f_magnitude, f_phase, f_kaver;
+    double f_k[3], f_re[3], f_im[3];
 } OracleParams;

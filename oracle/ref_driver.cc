@@ -11,6 +11,7 @@
  *   acHostReduceScal/Vec/VecScal   src/utils/modelreduce.cc:108-340
  *   acGetError                     src/utils/verification.cc:45-83
  *   acHostMeshWriteToFile/ReadFromFile  src/utils/memory.cc:182-247 (snapshot format)
+ *   helical_forcing_special_vector src/utils/astaroth_forcing.cc:158-216 (LFORCING build)
  * The two mesh helpers below stand in for src/core/astaroth.cc:324-335,425-431.
  */
 #include <stdlib.h>
@@ -95,6 +96,19 @@ make_mesh(double* const* fields, const int nx, const int ny, const int nz, const
         info[AC_mu0]        = p->mu0;
         info[AC_zeta]       = p->zeta;
         info[AC_K_heatcond] = p->K_heatcond;
+        info[AC_cs2_sound]  = p->cs_sound * p->cs_sound;
+        info[AC_forcing_magnitude] = p->f_magnitude;
+        info[AC_forcing_phase]     = p->f_phase;
+        info[AC_kaver]             = p->f_kaver;
+        info[AC_k_forcex]          = p->f_k[0];
+        info[AC_k_forcey]          = p->f_k[1];
+        info[AC_k_forcez]          = p->f_k[2];
+        info[AC_ff_hel_rex]        = p->f_re[0];
+        info[AC_ff_hel_rey]        = p->f_re[1];
+        info[AC_ff_hel_rez]        = p->f_re[2];
+        info[AC_ff_hel_imx]        = p->f_im[0];
+        info[AC_ff_hel_imy]        = p->f_im[1];
+        info[AC_ff_hel_imz]        = p->f_im[2];
     }
     for (int w = 0; w < NUM_VTXBUF_HANDLES; ++w)
         mesh.vertex_buffer[w] = fields[w];
@@ -175,3 +189,26 @@ ref_read_from_file(double* const* fields, const int nx, const int ny, const int 
     AcMesh mesh = make_mesh(fields, nx, ny, nz, NULL);
     return acHostMeshReadFromFile((size_t)id, &mesh) == AC_SUCCESS ? 0 : 1;
 }
+
+#if LFORCING
+/* src/utils/astaroth_forcing.cc:158-216, compiled into the LFORCING=1 build */
+void helical_forcing_special_vector(AcReal3* ff_hel_re, AcReal3* ff_hel_im, const AcReal3 k_force,
+                                    const AcReal3 e_force, const AcReal relhel);
+
+/* ff_hel_re and ff_hel_im of wave vector k and basis vector e */
+extern "C" void
+ref_forcing_special_vector(const double* k, const double* e, const double relhel, double* re,
+                           double* im)
+{
+    AcReal3 r, i;
+    helical_forcing_special_vector(&r, &i, (AcReal3){k[0], k[1], k[2]}, (AcReal3){e[0], e[1], e[2]},
+                                   relhel);
+    re[0] = r.x;
+    re[1] = r.y;
+    re[2] = r.z;
+    im[0] = i.x;
+    im[1] = i.y;
+    im[2] = i.z;
+}
+#endif
+

@@ -41,7 +41,9 @@ using std::isnan;
 #define LUPWD (0)
 #endif
 #define LBFIELD (0)
+#ifndef LFORCING /* the forcing variant of the model is built with -DLFORCING=1 */
 #define LFORCING (0)
+#endif
 #define LSHOCK (0)
 #define AC_LAGRANGIAN_GRID (0)
 #define AC_VERBOSE (0)
@@ -107,6 +109,20 @@ typedef enum {
     AC_mu0,
     AC_zeta,
     AC_K_heatcond,
+    /* used by the forcing of the LFORCING=1 build (modelsolver.cc:1031-1076) */
+    AC_cs2_sound,
+    AC_forcing_magnitude,
+    AC_forcing_phase,
+    AC_k_forcex,
+    AC_k_forcey,
+    AC_k_forcez,
+    AC_ff_hel_rex,
+    AC_ff_hel_rey,
+    AC_ff_hel_rez,
+    AC_ff_hel_imx,
+    AC_ff_hel_imy,
+    AC_ff_hel_imz,
+    AC_kaver,
     NUM_REAL_PARAMS
 } AcRealParam;
 typedef enum { AC_ds = 0, NUM_REAL3_PARAMS } AcReal3Param;

@@ -72,10 +72,25 @@ def test_python_enums_match_header():
     assert v["STREAM_ALL"] == capi.STREAM_ALL
 
 
-def test_struct_sizes():
-    # int_params[3] (12 B, padded to 16) + int3[8] (96) + real[16] (128) + real3[4] (96)
-    assert C.sizeof(capi.AcMeshInfo) == 12 + 96 + 4 + 128 + 96
-    assert C.sizeof(capi.AcReduction) == 5 * 4 + 4 + 8
+def test_struct_sizes_match_the_c_compiler(tmp_path):
+    """sizeof and member offsets of the ctypes mirrors equal those of the header
+    compiled by the C compiler."""
+    import subprocess
+
+    src = tmp_path / "sizes.c"
+    src.write_text('#include <stddef.h>\n#include <stdio.h>\n#include "astaroth_b200.h"\n'
+                   "int main(void) { printf(\"%zu %zu %zu %zu %zu %zu\\n\", sizeof(AcMeshInfo), "
+                   "offsetof(AcMeshInfo, int3_params), offsetof(AcMeshInfo, real_params), "
+                   "offsetof(AcMeshInfo, real3_params), sizeof(AcReduction), sizeof(AcMesh)); "
+                   "return 0; }\n")
+    exe = tmp_path / "sizes"
+    inc = Path(__file__).resolve().parents[1] / "include"
+    subprocess.run(["gcc", "-std=c11", f"-I{inc}", str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True,
+                                          check=True).stdout.split()]
+    M = capi.AcMeshInfo
+    assert got == [C.sizeof(M), M.int3_params.offset, M.real_params.offset,
+                   M.real3_params.offset, C.sizeof(capi.AcReduction), C.sizeof(capi.AcMesh)]
 
 
 def test_make_info_derived_params():
