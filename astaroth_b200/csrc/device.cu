@@ -694,16 +694,30 @@ launch_substep(Device d, cudaStream_t st, const int step, const double dt,
             return e;
         cfl = d->cfl;
     }
+    cudaError_t e;
     if (d->precision == 0) {
         const Fields64 f = fields64(d);
-        return tiled ? ac_launch_solve_tiled64(d->geom, &d->tmap[blk], f, sc, pc, rk, d->err_flag,
-                                               cfl, st, launches)
-                     : ac_launch_solve_plain64(d->geom, f, sc, pc, rk, cfl, st, launches);
+        e = tiled ? ac_launch_solve_tiled64(d->geom, &d->tmap[blk], f, sc, pc, rk, d->err_flag,
+                                            cfl, st, launches)
+                  : ac_launch_solve_plain64(d->geom, f, sc, pc, rk, cfl, st, launches);
     }
-    const Fields32 f = fields32(d);
-    return tiled ? ac_launch_solve_tiled32(d->geom, &d->tmap[blk], f, sc, pc, rk, d->err_flag, cfl,
-                                           st, launches)
-                 : ac_launch_solve_plain32(d->geom, f, sc, pc, rk, cfl, st, launches);
+    else {
+        const Fields32 f = fields32(d);
+        e = tiled ? ac_launch_solve_tiled32(d->geom, &d->tmap[blk], f, sc, pc, rk, d->err_flag,
+                                            cfl, st, launches)
+                  : ac_launch_solve_plain32(d->geom, f, sc, pc, rk, cfl, st, launches);
+    }
+    if (e != cudaSuccess || !pc.forcing)
+        return e;
+    /* helical forcing of the substep's output velocity */
+    void* u[3];
+    float* lo[3];
+    for (int c = 0; c < 3; ++c) {
+        const int q = VTXBUF_UUX + c, b = 1 - d->in_idx[q];
+        u[c]        = d->precision == 0 ? (void*)arr64(d, b, q) : (void*)arr_hi(d, b, q);
+        lo[c]       = d->precision == 0 ? nullptr : arr_lo(d, b, q);
+    }
+    return ac_launch_forcing(d->geom, u, lo, d->precision, pc, st, launches);
 }
 
 /* Periodic halo fill of the in-buffer of fields [q0, q0 + nq). */

@@ -233,6 +233,12 @@ cudaError_t ac_launch_solve_tiled32(const Geom& g, const void* tmap_in, const Fi
                                     int* err, unsigned long long* cfl, cudaStream_t stream,
                                     unsigned long long* launches);
 
+/* Helical forcing added to the three velocity arrays u (and their
+ * compensation arrays lo in FP32) after substep 2 (forcing.cu). */
+cudaError_t ac_launch_forcing(const Geom& g, void* const* u, float* const* lo, const int precision,
+                              const PhysConst& pc, cudaStream_t stream,
+                              unsigned long long* launches);
+
 /* CFL maxima of the in-buffer (cfl.cu); zeroes the three words first. */
 template <typename T>
 cudaError_t ac_launch_cfl(const Geom& g, const FieldsT<T>& f, const StencilCoef& sc,

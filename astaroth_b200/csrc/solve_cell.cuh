@@ -99,19 +99,12 @@ plain_cell(const Geom& g, const F& f, const StencilT<T>& sc, const PhysConst& pc
     }
 
     const T val[AC_NF] = {L.v, U.v[0], U.v[1], U.v[2], A.v[0], A.v[1], A.v[2], S.v};
-    /* helical forcing, added to u after its update (substep 2 launches only) */
-    T fu[3] = {0, 0, 0};
-    if (pc.forcing)
-        forcing_at(pc, i, j, k, fu);
 #pragma unroll
     for (int q = 0; q < AC_NF; ++q) {
-        const bool forced = pc.forcing && q >= VTXBUF_UUX && q <= VTXBUF_UUZ;
         if constexpr (COMP) {
             const RkT32 c = {(float)rk.dt, (float)rk.beta, (float)rk.ab};
             float oh, ol;
             rk_update_comp(val[q], lo[q], prev[q], prev_lo[q], r[q], c, use_prev, oh, ol);
-            if (forced)
-                comp_add(oh, ol, fu[q - VTXBUF_UUX]);
             f.out_p(q)[idx]    = oh;
             f.out_lo_p(q)[idx] = ol;
         }
@@ -119,8 +112,6 @@ plain_cell(const Geom& g, const F& f, const StencilT<T>& sc, const PhysConst& pc
             const RkT64 c = {rk.dt, rk.beta, rk.ab};
             double o;
             rk_update(val[q], prev[q], r[q], c, use_prev, o);
-            if (forced)
-                o += fu[q - VTXBUF_UUX];
             f.out_p(q)[idx] = o;
         }
     }

@@ -405,21 +405,13 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
                 val[2] = vd.v[2];
                 val[3] = sd.v;
             }
-            /* helical forcing of u (group 0, substep 2 launches only) */
-            T fu[3] = {0, 0, 0};
-            const bool forcing = pc.forcing && group == 0;
-            if (forcing)
-                forcing_at(pc, x, y, z, fu);
             /* group 0 writes lnrho, ux, uy, uz; group 1 writes ax, ay, az, entropy */
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                const bool forced = forcing && k >= 1;
                 if constexpr (COMP) {
                     const RkT32 c = {(float)rk.dt, (float)rk.beta, (float)rk.ab};
                     float oh, ol;
                     rk_update_comp(val[k], lo[k], prev[k], prevl[k], r[k], c, use_prev, oh, ol);
-                    if (forced)
-                        comp_add(oh, ol, fu[k - 1]);
                     outp[k][idx] = oh;
                     outl[k][idx] = ol;
                 }
@@ -427,8 +419,6 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
                     const RkT64 c = {rk.dt, rk.beta, rk.ab};
                     double o;
                     rk_update(val[k], prev[k], r[k], c, use_prev, o);
-                    if (forced)
-                        o += fu[k - 1];
                     outp[k][idx] = o;
                 }
             }
