@@ -264,6 +264,9 @@ SIGNATURES = {
                                               C.POINTER(AcMeshInfo)]),
     "acHostMeshWriteToFile": (C.c_int, [AcMesh, C.c_size_t]),
     "acHostMeshReadFromFile": (C.c_int, [C.c_size_t, C.POINTER(AcMesh)]),
+    "acDevicePlaneBytes": (C.c_size_t, [Device_p]),
+    "acDevicePackPlanes": (C.c_int, [Device_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "acDeviceUnpackPlanes": (C.c_int, [Device_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "acDeviceWriteMeshToDisk": (C.c_int, [Device_p, C.c_char_p, C.c_char_p, C.c_int]),
     "acDeviceReadMeshFromDisk": (C.c_int, [Device_p, C.c_char_p, C.c_char_p, C.c_int]),
     "acDeviceAdjointTapeForward": (C.c_int, [Device_p, C.c_int, C.c_int, C.c_double]),

@@ -175,8 +175,13 @@ forcing_for_launch(const AcMeshInfo& info, const double dt, PhysConst* pc)
         pc->f_re[a] = fre[a];
         pc->f_im[a] = fim[a];
     }
-    pc->f_cos_phase = cos(r[AC_forcing_phase]);
-    pc->f_sin_phase = sin(r[AC_forcing_phase]);
+    /* the kernel counts cells from this device's first interior cell; a slab
+     * of a larger grid starts at AC_multigpu_offset, which shifts the phase */
+    const int3 off    = info.int3_params[AC_multigpu_offset];
+    const double ph   = r[AC_forcing_phase] + pc->f_k[0] * off.x + pc->f_k[1] * off.y +
+                      pc->f_k[2] * off.z;
+    pc->f_cos_phase = cos(ph);
+    pc->f_sin_phase = sin(ph);
     /* N = cs magnitude sqrt(kaver cs); the force is sqrt(dt) N f */
     const double cs = sqrt(r[AC_cs_sound] * r[AC_cs_sound]);
     pc->f_scale     = sqrt(dt) * cs * r[AC_forcing_magnitude] * sqrt(r[AC_kaver] * cs);
@@ -1309,6 +1314,67 @@ acDeviceGetParamAdjoints(const Device d, AcReal* nu_bar, AcReal* eta_bar)
     *nu_bar  = v[0];
     *eta_bar = v[1];
     return AC_SUCCESS;
+}
+
+/* ---- whole-plane copies for a z-slab decomposition ----
+ * The halo exchange of the reference's grid layer packs boundary slabs into
+ * buffers and unpacks them into the neighbours' ghost zones
+ * (src/core/kernels/packing.cuh:59-470, src/core/task.cc:1933-1993).  With a
+ * decomposition along z only, a z halo is a run of whole xy planes, contiguous
+ * in every field array, so packing is one copy per array: the buffer holds, for
+ * each array (the 8 value arrays, then the 8 compensation arrays of FP32
+ * meshes), `nplanes` planes of px*my elements. */
+static bool
+planes_ok(const Device d, const int z0, const int nplanes)
+{
+    return d && nplanes > 0 && z0 >= 0 && z0 + nplanes <= d->geom.mz;
+}
+
+static int
+plane_arrays(const Device d)
+{
+    return d->precision == 0 ? AC_NF : 2 * AC_NF;
+}
+
+extern "C" size_t
+acDevicePlaneBytes(const Device d)
+{
+    return d ? (size_t)d->geom.pxy * elem_size(d) * plane_arrays(d) : 0;
+}
+
+static AcResult
+copy_planes(const Device d, const Stream stream, const int z0, const int nplanes, char* buffer,
+            const bool pack)
+{
+    if (!planes_ok(d, z0, nplanes) || !buffer || !stream_ok(stream))
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    const size_t es    = elem_size(d);
+    const size_t bytes = (size_t)nplanes * d->geom.pxy * es;
+    for (int a = 0; a < plane_arrays(d); ++a) {
+        const int q = a % AC_NF;
+        char* arr   = a < AC_NF ? (char*)d->hi[d->in_idx[q]] + (size_t)q * d->geom.cells * es
+                                : (char*)arr_lo(d, d->in_idx[q], q);
+        char* field = arr + (size_t)z0 * d->geom.pxy * es;
+        char* buf   = buffer + (size_t)a * bytes;
+        AC_CUDA_CHECK(cudaMemcpyAsync(pack ? buf : field, pack ? field : buf, bytes,
+                                      cudaMemcpyDeviceToDevice, d->streams[stream]));
+    }
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDevicePackPlanes(const Device d, const Stream stream, const int z0, const int nplanes,
+                   void* buffer)
+{
+    return copy_planes(d, stream, z0, nplanes, (char*)buffer, true);
+}
+
+extern "C" AcResult
+acDeviceUnpackPlanes(const Device d, const Stream stream, const int z0, const int nplanes,
+                     const void* buffer)
+{
+    return copy_planes(d, stream, z0, nplanes, (char*)buffer, false);
 }
 
 /* ---- snapshots of the computational domain: src/core/grid.cc:3792-3935 ----

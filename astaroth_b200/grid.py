@@ -1,0 +1,261 @@
+"""A periodic mesh decomposed along z into slabs, one Device per slab: the
+grid layer of the reference (acGridInit / acGridIntegrate /
+acGridPeriodicBoundconds / acGridReduceScal, src/core/grid.cc:3086-3110,
+3170-3230; halo exchange src/core/task.cc:1933-1993; CFL allreduce
+task.cc:2865-2882) for slab decompositions.
+
+One RK3 substep of the grid is, on every slab:
+
+1. the periodic fill of the x and y ghost zones of the interior z planes
+   (acDevicePeriodicBoundconds on the box [0, mx) x [0, my) x [3, nz + 3));
+2. the exchange of the three bottom and three top interior planes of every
+   field with the slabs below and above (whole xy planes, halo rows and columns
+   included, so edges and corners are right): acDevicePackPlanes into a send
+   buffer, a transport, acDeviceUnpackPlanes into the ghost planes;
+3. acDeviceIntegrateSubstep and the buffer swap.
+
+Transports:
+
+* ``LocalTransport`` -- every slab in this process, on one GPU; the exchange
+  is device-to-device copies.  It exercises the decomposition on one GPU and
+  gives the same bits as an undecomposed Device.
+* ``DistTransport`` -- one slab per rank of a torch.distributed process group
+  (NCCL between GPUs, gloo on CPU tensors): point-to-point sends of the packed
+  planes to the ranks below and above.
+
+Reductions combine the slabs' unprocessed results (max, min, sum) and apply the
+RMS post-processing with the global cell count; the CFL maxima are combined
+with max before the timestep formula.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import capi
+from .capi import AcMeshInfo, Int3Param, Volume
+from .device import AstarothError, Device, _check, dims, make_info
+
+HALO = capi.NGHOST
+
+
+def decompose(nz: int, parts: int) -> list[tuple[int, int]]:
+    """(z0, nz) of each of `parts` slabs covering nz planes, sizes differing by
+    at most one (the first nz % parts slabs one plane larger)."""
+    if parts < 1 or nz < parts * HALO:
+        raise ValueError(f"{nz} planes cannot be split into {parts} slabs of >= {HALO} planes")
+    base, extra = divmod(nz, parts)
+    out, z0 = [], 0
+    for p in range(parts):
+        n = base + (1 if p < extra else 0)
+        out.append((z0, n))
+        z0 += n
+    return out
+
+
+def slab_info(info: AcMeshInfo, z0: int, nz: int) -> AcMeshInfo:
+    """The AcMeshInfo of one slab: AC_nlocal = (nx, ny, nz) with the global
+    AC_ngrid and AC_ds, AC_multigpu_offset = (0, 0, z0)."""
+    s = AcMeshInfo()
+    C.memmove(C.byref(s), C.byref(info), C.sizeof(AcMeshInfo))
+    n = s.int3_params[Int3Param.AC_ngrid]
+    s.int3_params[Int3Param.AC_nlocal] = capi.Int3(n.x, n.y, nz)
+    s.int3_params[Int3Param.AC_multigpu_offset] = capi.Int3(0, 0, z0)
+    _check(capi.load().acHostUpdateParams(C.byref(s)), "acHostUpdateParams")
+    return s
+
+
+class LocalTransport:
+    """All slabs in this process: slab i's bottom ghost planes come from slab
+    i - 1's top interior planes and its top ghost planes from slab i + 1's
+    bottom interior planes (periodically)."""
+
+    def exchange(self, send_bottom, send_top, recv_bottom, recv_top):
+        k = len(send_bottom)
+        for i in range(k):
+            recv_bottom[i].copy_(send_top[(i - 1) % k])
+            recv_top[i].copy_(send_bottom[(i + 1) % k])
+
+    def combine(self, values, op):
+        return {"max": max, "min": min, "sum": math.fsum}[op](values)
+
+
+class DistTransport:
+    """One slab per rank: the top planes go to rank + 1 (its bottom ghost), the
+    bottom planes to rank - 1 (its top ghost), periodically.  Sends and
+    receives are posted in the same order on every rank, so messages between
+    the same two ranks match in order (world size 2 has one neighbour on both
+    sides)."""
+
+    def __init__(self):
+        import torch.distributed as dist
+
+        self.dist = dist
+        self.rank = dist.get_rank()
+        self.world = dist.get_world_size()
+
+    def exchange(self, send_bottom, send_top, recv_bottom, recv_top):
+        (sb,), (st,), (rb,), (rt,) = send_bottom, send_top, recv_bottom, recv_top
+        if self.world == 1:
+            rb.copy_(st)
+            rt.copy_(sb)
+            return
+        d = self.dist
+        up, down = (self.rank + 1) % self.world, (self.rank - 1) % self.world
+        reqs = [d.isend(st, up, tag=1), d.irecv(rb, down, tag=1),
+                d.isend(sb, down, tag=2), d.irecv(rt, up, tag=2)]
+        for r in reqs:
+            r.wait()
+
+    def combine(self, values, op):
+        import torch
+
+        (v,) = values
+        t = torch.tensor([v], dtype=torch.float64,
+                         device="cuda" if self.dist.get_backend() == "nccl" else "cpu")
+        red = {"max": self.dist.ReduceOp.MAX, "min": self.dist.ReduceOp.MIN,
+               "sum": self.dist.ReduceOp.SUM}[op]
+        self.dist.all_reduce(t, op=red)
+        return float(t.item())
+
+
+class Grid:
+    """A periodic mesh of global size AC_ngrid split into z slabs.
+
+    info: the global AcMeshInfo.  With ``transport=None`` the mesh is split into
+    ``slabs`` slabs held in this process (LocalTransport); with a DistTransport
+    this process holds its rank's slab of ``world`` slabs.
+    """
+
+    def __init__(self, info: AcMeshInfo, slabs: int = 1, transport=None, device_id: int = 0):
+        import torch
+
+        self.lib = capi.load()
+        self.info = info
+        self.n = dims(info)
+        nz = self.n[2]
+        if isinstance(transport, DistTransport):
+            self.ranges = [decompose(nz, transport.world)[transport.rank]]
+        else:
+            transport = transport or LocalTransport()
+            self.ranges = decompose(nz, slabs)
+        self.transport = transport
+        self.devs = [Device(slab_info(info, z0, n), device_id) for z0, n in self.ranges]
+        self.plane_bytes = self.lib.acDevicePlaneBytes(self.devs[0].handle)
+        dev = torch.device("cuda", device_id)
+        self._buf = {k: [torch.empty(HALO * self.plane_bytes, dtype=torch.uint8, device=dev)
+                         for _ in self.devs] for k in ("sb", "st", "rb", "rt")}
+        self.cells = self.n[0] * self.n[1] * self.n[2]
+
+    def destroy(self):
+        for d in self.devs:
+            d.destroy()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.destroy()
+
+    # ---- data ----
+    def load_mesh(self, fields: np.ndarray) -> None:
+        """Loads this process's slabs from a global (8, mz, my, mx) mesh."""
+        for d, (z0, n) in zip(self.devs, self.ranges):
+            d.load_mesh(np.ascontiguousarray(fields[:, z0:z0 + n + 2 * HALO]))
+
+    def store_mesh(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The interior planes of this process's slabs in a global (8, mz, my, mx)
+        array (cells of other ranks' slabs and ghost planes are left as they are)."""
+        nx, ny, nz = self.n
+        if out is None:
+            out = np.zeros((capi.NUM_FIELDS, nz + 2 * HALO, ny + 2 * HALO, nx + 2 * HALO))
+        for d, (z0, n) in zip(self.devs, self.ranges):
+            s = d.store_mesh()
+            out[:, HALO + z0:HALO + z0 + n] = s[:, HALO:HALO + n]
+        return out
+
+    # ---- boundary conditions ----
+    def periodic_boundconds(self) -> None:
+        """Fills every ghost cell of every slab: x and y by local wrap, z by the
+        exchange with the neighbouring slabs."""
+        import torch
+
+        for d, (_, n) in zip(self.devs, self.ranges):
+            nx, ny, _ = self.n
+            _check(self.lib.acDevicePeriodicBoundconds(
+                d.handle, 0, Volume(0, 0, HALO), Volume(nx + 2 * HALO, ny + 2 * HALO, n + HALO)),
+                "acDevicePeriodicBoundconds")
+        b = self._buf
+        for i, (d, (_, n)) in enumerate(zip(self.devs, self.ranges)):
+            _check(self.lib.acDevicePackPlanes(d.handle, 0, HALO, HALO, b["sb"][i].data_ptr()),
+                   "acDevicePackPlanes")
+            _check(self.lib.acDevicePackPlanes(d.handle, 0, n, HALO, b["st"][i].data_ptr()),
+                   "acDevicePackPlanes")
+        for d in self.devs:
+            d.synchronize(0)
+        self.transport.exchange(b["sb"], b["st"], b["rb"], b["rt"])
+        torch.cuda.current_stream().synchronize()
+        for i, (d, (_, n)) in enumerate(zip(self.devs, self.ranges)):
+            _check(self.lib.acDeviceUnpackPlanes(d.handle, 0, 0, HALO, b["rb"][i].data_ptr()),
+                   "acDeviceUnpackPlanes")
+            _check(self.lib.acDeviceUnpackPlanes(d.handle, 0, n + HALO, HALO,
+                                                 b["rt"][i].data_ptr()), "acDeviceUnpackPlanes")
+
+    # ---- integration ----
+    def integrate_substep(self, step: int, dt: float) -> None:
+        self.periodic_boundconds()
+        for d in self.devs:
+            d.integrate_substep(step, dt)
+        for d in self.devs:
+            d.swap_buffers()
+
+    def integrate_step(self, dt: float) -> None:
+        for s in range(3):
+            self.integrate_substep(s, dt)
+
+    def synchronize(self) -> None:
+        for d in self.devs:
+            d.synchronize()
+
+    # ---- reductions over the whole grid ----
+    def _post(self, rtype: str, v: float) -> float:
+        r = capi.RTYPES[rtype]
+        if r.post_processing_op == 1:  # AC_RMS: sqrt(sum / cells) over the global grid
+            return math.sqrt(v / self.cells)
+        return v
+
+    def _op(self, rtype: str) -> str:
+        return {capi.ReduceOp.AC_REDUCE_OP_MAX: "max", capi.ReduceOp.AC_REDUCE_OP_MIN: "min",
+                capi.ReduceOp.AC_REDUCE_OP_SUM: "sum"}[capi.RTYPES[rtype].reduce_op]
+
+    def reduce_scal(self, rtype: str, field: int) -> float:
+        vals = [d.reduce_scal(rtype, field, post=False) for d in self.devs]
+        return self._post(rtype, self.transport.combine([self._local(vals, rtype)],
+                                                        self._op(rtype)))
+
+    def reduce_vec(self, rtype: str, a: int, b: int, c: int) -> float:
+        vals = [d.reduce_vec(rtype, a, b, c, post=False) for d in self.devs]
+        return self._post(rtype, self.transport.combine([self._local(vals, rtype)],
+                                                        self._op(rtype)))
+
+    def _local(self, vals, rtype):
+        op = self._op(rtype)
+        return {"max": max, "min": min, "sum": math.fsum}[op](vals)
+
+    # ---- CFL timestep ----
+    def calc_timestep(self) -> None:
+        for d in self.devs:
+            d.calc_timestep()
+
+    def timestep(self) -> float:
+        """dt from the CFL maxima of all slabs (the last substep 2, or
+        calc_timestep), combined with max as the reference's allreduce."""
+        us, vs = zip(*(d.timestep_maxima() for d in self.devs))
+        u = self.transport.combine([max(us)], "max")
+        va = self.transport.combine([max(vs)], "max")
+        return self.lib.acHostTimestepFromMaxima(self.info, u, va)
+
+
+__all__ = ["Grid", "LocalTransport", "DistTransport", "decompose", "slab_info"]

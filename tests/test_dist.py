@@ -4,6 +4,7 @@ of independent members across ranks (no data-path collective)."""
 import os
 import socket
 
+import pytest
 import torch.multiprocessing as mp
 
 from astaroth_b200 import dist as adist
@@ -66,3 +67,62 @@ def test_single_process_defaults():
     assert adist.max_over_ranks(3.5) == 3.5
     assert adist.sum_over_ranks(2.0) == 2.0
     adist.barrier()
+
+
+def _exchange_worker(rank, world, port, out):
+    import torch
+
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    assert adist.init("gloo", timeout_s=60)
+    from astaroth_b200.grid import DistTransport
+
+    t = DistTransport()
+    n = 64
+    sb = torch.full((n,), 10 * rank + 1, dtype=torch.uint8)
+    st = torch.full((n,), 10 * rank + 2, dtype=torch.uint8)
+    rb = torch.zeros(n, dtype=torch.uint8)
+    rt = torch.zeros(n, dtype=torch.uint8)
+    for _ in range(3):  # repeated exchanges keep matching in order
+        t.exchange([sb], [st], [rb], [rt])
+    res = (rank, int(rb[0]), int(rb[-1]), int(rt[0]), int(rt[-1]),
+           t.combine([float(rank + 1)], "max"), t.combine([float(rank + 1)], "min"),
+           t.combine([float(rank + 1)], "sum"))
+    out.put(res)
+    adist.barrier()
+    adist.destroy()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_grid_halo_exchange_gloo(world):
+    """Each rank's bottom ghost receives the top planes of the rank below and
+    its top ghost the bottom planes of the rank above, periodically; the
+    reductions combine over the ranks."""
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_exchange_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in range(world))
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    for rank, rb0, rb1, rt0, rt1, mx, mn, sm in res:
+        below, above = (rank - 1) % world, (rank + 1) % world
+        assert rb0 == rb1 == 10 * below + 2
+        assert rt0 == rt1 == 10 * above + 1
+        assert (mx, mn, sm) == (world, 1, world * (world + 1) / 2)
+
+
+def test_decompose_covers_the_planes():
+    from astaroth_b200.grid import decompose
+
+    for nz, parts in ((48, 2), (20, 3), (16, 5), (9, 3)):
+        r = decompose(nz, parts)
+        assert r[0][0] == 0 and sum(n for _, n in r) == nz
+        assert all(r[i][0] + r[i][1] == r[i + 1][0] for i in range(parts - 1))
+        assert max(n for _, n in r) - min(n for _, n in r) <= 1
+        assert min(n for _, n in r) >= 3
+    with pytest.raises(ValueError):
+        decompose(8, 3)  # slabs thinner than the 3-plane halo

@@ -1,0 +1,113 @@
+"""The z-slab grid (astaroth_b200.grid) on one GPU: the mesh split into 1-4
+slabs in one process (LocalTransport), or one slab in a process group of one
+rank (DistTransport over NCCL), gives the same bits as one undecomposed Device
+after whole RK3 steps; global reductions and the CFL timestep agree."""
+import ctypes as C
+import os
+import socket
+
+import numpy as np
+import pytest
+
+from astaroth_b200 import capi
+from astaroth_b200.capi import IntParam, Real3
+from astaroth_b200.device import CONFIG_PARAMS, Device, make_info, seeded_mesh
+from astaroth_b200.grid import DistTransport, Grid
+
+pytestmark = pytest.mark.gpu
+
+DT = 1e-3
+
+
+def _device(info, f, steps):
+    with Device(info) as d:
+        d.load_mesh(f)
+        for _ in range(steps):
+            d.integrate_step(DT)
+        d.synchronize()
+        return d.store_mesh()
+
+
+def _interior(a):
+    return a[:, 3:-3, 3:-3, 3:-3]
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("shape,slabs", [((40, 36, 48), 2), ((32, 32, 20), 3), ((40, 36, 48), 4),
+                                         ((33, 24, 16), 1)])
+def test_slabs_equal_one_device(shape, slabs, precision):
+    info = make_info(shape, precision=precision)
+    f = seeded_mesh(info, 81)
+    with Grid(info, slabs=slabs) as g:
+        g.load_mesh(f)
+        for _ in range(3):
+            g.integrate_step(DT)
+        g.synchronize()
+        got = g.store_mesh()
+    assert np.array_equal(_interior(got), _interior(_device(info, f, 3)))
+
+
+def test_reductions_and_timestep():
+    info = make_info((40, 36, 30))
+    f = seeded_mesh(info, 82, sigma_uu=1e-2)
+    with Grid(info, slabs=3) as g, Device(info) as d:
+        g.load_mesh(f)
+        d.load_mesh(f)
+        g.integrate_step(DT)
+        d.integrate_step(DT)
+        for rt in ("RTYPE_MAX", "RTYPE_MIN"):
+            assert g.reduce_scal(rt, 2) == d.reduce_scal(rt, 2)
+            assert g.reduce_vec(rt, 1, 2, 3) == d.reduce_vec(rt, 1, 2, 3)
+        for rt in ("RTYPE_RMS", "RTYPE_SUM", "RTYPE_RMS_EXP"):
+            assert g.reduce_scal(rt, 0) == pytest.approx(d.reduce_scal(rt, 0), rel=1e-13)
+        # the maxima of the last substep 2, combined over the slabs with max
+        assert g.timestep() == d.timestep()
+
+
+def test_forcing_across_slabs():
+    """The forcing phase of each slab is shifted by its z offset."""
+    info = make_info((32, 32, 24), **dict(CONFIG_PARAMS, relhel=0.5, forcing_magnitude=0.5,
+                                           kmin=0.8, kmax=2.2, current_time=1.0))
+    info.int_params[IntParam.AC_lforcing] = 1
+    assert capi.load().acHostForcingParams(Real3(1, 0, 1), 0.4, 0.7, C.byref(info)) == 0
+    f = seeded_mesh(info, 83)
+    with Grid(info, slabs=3) as g:
+        g.load_mesh(f)
+        g.integrate_step(DT)
+        g.synchronize()
+        got = g.store_mesh()
+    ref = _device(info, f, 1)
+    err = np.abs(_interior(got) - _interior(ref)).max() / np.abs(_interior(ref)).max()
+    assert err <= 1e-13
+
+
+def test_dist_transport_one_rank():
+    import torch.distributed as dist
+
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("nccl", rank=0, world_size=1)
+    try:
+        info = make_info((32, 28, 24))
+        f = seeded_mesh(info, 84)
+        with Grid(info, transport=DistTransport()) as g:
+            g.load_mesh(f)
+            for _ in range(2):
+                g.integrate_step(DT)
+            g.synchronize()
+            got = g.store_mesh()
+            assert g.reduce_scal("RTYPE_MAX", 1) == _device_max(info, f)
+        assert np.array_equal(_interior(got), _interior(_device(info, f, 2)))
+    finally:
+        dist.destroy_process_group()
+
+
+def _device_max(info, f):
+    with Device(info) as d:
+        d.load_mesh(f)
+        for _ in range(2):
+            d.integrate_step(DT)
+        return d.reduce_scal("RTYPE_MAX", 1)
