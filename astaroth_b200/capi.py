@@ -191,7 +191,8 @@ Ensemble_p = C.c_void_p
 
 
 class AcEnsembleTiles(C.Structure):
-    _fields_ = [("tx", C.c_int), ("ty", C.c_int), ("zb", C.c_int), ("blocks_per_sm", C.c_int)]
+    _fields_ = [("tx", C.c_int), ("ty", C.c_int), ("zb", C.c_int), ("blocks_per_sm", C.c_int),
+                ("mode", C.c_int)]
 
 # name -> (restype, argtypes)
 SIGNATURES = {

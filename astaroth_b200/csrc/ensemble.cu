@@ -171,6 +171,13 @@ struct ensemble_s {
     ReduceScratch red;
     double* host_result;
     unsigned long long launches;
+    /* mode 1: per-member tensor maps of both buffer parities, branch streams */
+    std::vector<CUtensorMap> tmaps; /* 2 per member: [2 m + parity] */
+    std::vector<char> tiled;        /* member fits the tiled kernel (else: plain) */
+    std::vector<cudaStream_t> branches;
+    std::vector<cudaEvent_t> joins;
+    cudaEvent_t fork;
+    int* err;
 };
 
 namespace {
@@ -208,7 +215,14 @@ destroy(Ensemble e)
     cudaFree(e->items);
     cudaFree(e->staging);
     cudaFree(e->red.partials);
+    cudaFree(e->err);
     cudaFreeHost(e->host_result);
+    for (cudaStream_t b : e->branches)
+        cudaStreamDestroy(b);
+    for (cudaEvent_t j : e->joins)
+        cudaEventDestroy(j);
+    if (e->fork)
+        cudaEventDestroy(e->fork);
     if (e->stream)
         cudaStreamDestroy(e->stream);
     free(e->hmem);
@@ -319,7 +333,7 @@ tiles_ok(const AcEnsembleTiles t)
 {
     const int threads = t.tx * t.ty;
     return t.tx >= 1 && t.ty >= 1 && t.zb >= 1 && threads <= 256 && threads % 32 == 0 &&
-           t.blocks_per_sm >= 0;
+           t.blocks_per_sm >= 0 && (t.mode == 0 || t.mode == 1);
 }
 
 cudaError_t
@@ -357,9 +371,82 @@ launch_halo(Ensemble e, unsigned long long* launches)
     return cudaGetLastError();
 }
 
+/* Mode 1: the substeps [s0, s1) of every member as tiled single-mesh launches,
+ * member chains spread over the branch streams, which fork from and join into
+ * the ensemble stream (so a capture of the ensemble stream records them as
+ * concurrent branches).  The in-block parity of substep s is parity ^ (s & 1)
+ * relative to s0. */
+template <typename T, bool COMP>
+cudaError_t
+record_members(Ensemble e, const int s0, const int s1, unsigned long long* launches,
+               const bool halo = true)
+{
+    cudaError_t err = cudaEventRecord(e->fork, e->stream);
+    if (err != cudaSuccess)
+        return err;
+    const int nb = (int)e->branches.size();
+    for (int b = 0; b < nb; ++b) {
+        err = cudaStreamWaitEvent(e->branches[b], e->fork, 0);
+        if (err != cudaSuccess)
+            return err;
+    }
+    const Volume m0 = {0, 0, 0};
+    for (int m = 0; m < e->n; ++m) {
+        cudaStream_t st       = e->branches[m % nb];
+        const EnsMember<T>& r = members<T>(e)[m];
+        const Volume m1       = {(size_t)r.g.mx, (size_t)r.g.my, (size_t)r.g.mz};
+        for (int s = s0; s < s1; ++s) {
+            const int p         = e->parity ^ ((s - s0) & 1);
+            const FieldsT<T>& f = r.f[p];
+            T* arr[2 * AC_NF];
+            for (int q = 0; q < AC_NF; ++q) {
+                arr[q]         = const_cast<T*>(f.in[q]);
+                arr[AC_NF + q] = COMP ? const_cast<T*>(f.in_lo[q]) : nullptr;
+            }
+            if (halo) {
+                err = ac_launch_periodic<T>(r.g, arr, COMP ? 2 * AC_NF : AC_NF, m0, m1, st,
+                                            launches);
+                if (err != cudaSuccess)
+                    return err;
+            }
+            const RkCoef rk     = ac_rk_coef(s, e->dts[m]);
+            const void* tmap    = &e->tmaps[2 * m + p];
+            /* the kernel a Device of this member would use */
+            if constexpr (COMP)
+                err = e->tiled[m] ? ac_launch_solve_tiled32(r.g, tmap, f, e->sc[m], e->pc[m], rk,
+                                                            e->err, nullptr, st, launches)
+                                  : ac_launch_solve_plain32(r.g, f, e->sc[m], e->pc[m], rk, nullptr,
+                                                            st, launches);
+            else
+                err = e->tiled[m] ? ac_launch_solve_tiled64(r.g, tmap, f, e->sc[m], e->pc[m], rk,
+                                                            e->err, nullptr, st, launches)
+                                  : ac_launch_solve_plain64(r.g, f, e->sc[m], e->pc[m], rk, nullptr,
+                                                            st, launches);
+            if (err != cudaSuccess)
+                return err;
+        }
+    }
+    for (int b = 0; b < nb; ++b) {
+        err = cudaEventRecord(e->joins[b], e->branches[b]);
+        if (err != cudaSuccess)
+            return err;
+        err = cudaStreamWaitEvent(e->stream, e->joins[b], 0);
+        if (err != cudaSuccess)
+            return err;
+    }
+    return cudaSuccess;
+}
+
 cudaError_t
 record_step(Ensemble e, unsigned long long* launches)
 {
+    if (e->tiles.mode == 1) {
+        const cudaError_t err = e->precision == 0 ? record_members<double, false>(e, 0, 3, launches)
+                                                  : record_members<float, true>(e, 0, 3, launches);
+        if (err == cudaSuccess)
+            e->parity ^= 1; /* three swaps */
+        return err;
+    }
     for (int s = 0; s < 3; ++s) {
         cudaError_t err = launch_halo(e, launches);
         if (err != cudaSuccess)
@@ -588,8 +675,29 @@ acEnsembleCreate(const int device_id, const int n, const AcMeshInfo* configs, En
     e->red.counter = (unsigned int*)(e->red.result + 2);
     ENS_CHECK(cudaMallocHost((void**)&e->host_result, sizeof(double)));
     ENS_CHECK(cudaStreamSynchronize(e->stream));
-    const AcEnsembleTiles def = {32, 4, 8, 0};
+    const AcEnsembleTiles def = {32, 4, 8, 0, 0};
     ENS_CHECK(build_items(e, def));
+    /* mode 1: tensor maps of both buffer blocks of every member, branch streams */
+    ENS_CHECK(cudaMalloc((void**)&e->err, sizeof(int)));
+    ENS_CHECK(cudaMemset(e->err, 0, sizeof(int)));
+    e->tmaps.resize(2 * (size_t)n);
+    e->tiled.assign(n, 1);
+    for (int m = 0; m < n; ++m)
+        for (int p = 0; p < 2; ++p) {
+            void* base = e->precision == 0 ? (void*)members<double>(e)[m].f[p].in[0]
+                                           : (void*)members<float>(e)[m].f[p].in[0];
+            if (!ac_make_tensor_map(&e->tmaps[2 * m + p], base, e->geom[m], e->precision))
+                e->tiled[m] = 0;
+        }
+    ENS_CHECK(ac_solve_tiled_init(e->precision));
+    const int nb = std::min(n, 16);
+    e->branches.assign(nb, nullptr);
+    e->joins.assign(nb, nullptr);
+    for (int b = 0; b < nb; ++b) {
+        ENS_CHECK(cudaStreamCreateWithFlags(&e->branches[b], cudaStreamNonBlocking));
+        ENS_CHECK(cudaEventCreateWithFlags(&e->joins[b], cudaEventDisableTiming));
+    }
+    ENS_CHECK(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
 #undef ENS_CHECK
     *out = e;
     return AC_SUCCESS;
@@ -686,6 +794,7 @@ acEnsembleSetTimesteps(const Ensemble e, const AcReal* dts)
     AC_CUDA_CHECK(cudaMemcpyAsync(e->d_dts, e->dts.data(), e->n * sizeof(double),
                                   cudaMemcpyHostToDevice, e->stream));
     AC_CUDA_CHECK(cudaStreamSynchronize(e->stream));
+    invalidate(e); /* mode 1 launches take dt as a parameter */
     return AC_SUCCESS;
 }
 
@@ -696,7 +805,13 @@ acEnsembleIntegrateStep(const Ensemble e)
         return AC_FAILURE;
     AC_CUDA_CHECK(cudaSetDevice(e->id));
     const int p = e->parity;
-    if (!e->graph_valid[p]) {
+    /* capture the graphs of both buffer parities at the first step, so later
+     * steps (which alternate parities) never capture */
+    for (int c = 0; c < 2; ++c) {
+        const int pc = p ^ c;
+        if (e->graph_valid[pc])
+            continue;
+        e->parity = pc;
         cudaGraph_t graph;
         AC_CUDA_CHECK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
         const cudaError_t rec = record_step(e, NULL);
@@ -704,13 +819,13 @@ acEnsembleIntegrateStep(const Ensemble e)
         e->parity             = p; /* undo the capture's swaps */
         AC_CUDA_CHECK(rec);
         AC_CUDA_CHECK(end);
-        const cudaError_t inst = cudaGraphInstantiate(&e->graph[p], graph, 0);
+        const cudaError_t inst = cudaGraphInstantiate(&e->graph[pc], graph, 0);
         cudaGraphDestroy(graph);
         AC_CUDA_CHECK(inst);
-        e->graph_valid[p] = 1;
+        e->graph_valid[pc] = 1;
     }
     AC_CUDA_CHECK(cudaGraphLaunch(e->graph[p], e->stream));
-    e->launches += 6;
+    e->launches += e->tiles.mode == 1 ? 6ull * e->n : 6ull; /* halo + solve, 3 substeps */
     e->parity ^= 1; /* three swaps */
     return AC_SUCCESS;
 }
@@ -761,7 +876,7 @@ acEnsembleAutotune(const Ensemble e, AcEnsembleTiles* best, double* best_ms)
     std::vector<AcEnsembleTiles> cand;
     for (const auto& s : shapes)
         for (const int zb : zbs)
-            cand.push_back({s[0], s[1], zb, 0});
+            cand.push_back({s[0], s[1], zb, 0, 0});
     cudaEvent_t t0, t1;
     AC_CUDA_CHECK(cudaEventCreate(&t0));
     AC_CUDA_CHECK(cudaEventCreate(&t1));
@@ -813,9 +928,54 @@ acEnsembleAutotune(const Ensemble e, AcEnsembleTiles* best, double* best_ms)
             win    = t;
         }
     }
+    /* then the two modes on the solve of substep 0 (no halo fill, so the state
+     * is left as it was), each replayed from a captured graph */
+    auto time_graph = [&](const int mode, double* ms) -> cudaError_t {
+        cudaGraph_t graph;
+        cudaGraphExec_t exec;
+        cudaError_t rec = cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal);
+        if (rec != cudaSuccess)
+            return rec;
+        if (mode == 0)
+            rec = launch_solve(e, 0, NULL);
+        else
+            rec = e->precision == 0 ? record_members<double, false>(e, 0, 1, NULL, false)
+                                    : record_members<float, true>(e, 0, 1, NULL, false);
+        const cudaError_t end = cudaStreamEndCapture(e->stream, &graph);
+        if (rec != cudaSuccess)
+            return rec;
+        if (end != cudaSuccess)
+            return end;
+        cudaError_t r = cudaGraphInstantiate(&exec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (r != cudaSuccess)
+            return r;
+        const int reps = 5;
+        r              = cudaGraphLaunch(exec, e->stream);
+        cudaEventRecord(t0, e->stream);
+        for (int k = 0; k < reps && r == cudaSuccess; ++k)
+            r = cudaGraphLaunch(exec, e->stream);
+        cudaEventRecord(t1, e->stream);
+        if (r == cudaSuccess)
+            r = cudaEventSynchronize(t1);
+        float f = 0;
+        cudaEventElapsedTime(&f, t0, t1);
+        *ms = f / reps;
+        cudaGraphExecDestroy(exec);
+        return r;
+    };
+    if (err == cudaSuccess)
+        err = build_items(e, win);
+    double ms0 = 0, ms1 = 1e300;
+    if (err == cudaSuccess)
+        err = time_graph(0, &ms0);
+    if (err == cudaSuccess)
+        err = time_graph(1, &ms1);
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);
     AC_CUDA_CHECK(err);
+    win.mode = ms1 < ms0 ? 1 : 0;
+    win_ms   = ms1 < ms0 ? ms1 : ms0;
     AC_CUDA_CHECK(build_items(e, win));
     if (best)
         *best = win;

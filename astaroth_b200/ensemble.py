@@ -7,9 +7,11 @@ graph.  Each member's cells follow the arithmetic of a single-mesh Device
 without tiling, so a member's result equals that Device's bit for bit.
 
 The tile shape of the persistent launch comes from ``Ensemble.autotune``: the
-library times a fixed candidate set on the current members and keeps the
-fastest; the result can be cached in a JSON file keyed by the member sizes,
-the precision and the GPU name.
+library times a fixed candidate set on the current members, then compares a
+whole substep of the best persistent launch with mode 1 (one shared-memory
+tiled launch per member, the members' launches as concurrent graph branches)
+and keeps the faster; the result can be cached in a JSON file keyed by the
+member sizes, the precision and the GPU name.
 """
 from __future__ import annotations
 
@@ -126,10 +128,13 @@ class Ensemble:
     def tiles(self) -> tuple:
         t = AcEnsembleTiles()
         _check(self.lib.acEnsembleGetTiles(self._h, C.byref(t)), "acEnsembleGetTiles")
-        return (t.tx, t.ty, t.zb, t.blocks_per_sm)
+        return (t.tx, t.ty, t.zb, t.blocks_per_sm, t.mode)
 
-    def set_tiles(self, tx: int, ty: int, zb: int, blocks_per_sm: int = 0) -> None:
-        _check(self.lib.acEnsembleSetTiles(self._h, AcEnsembleTiles(tx, ty, zb, blocks_per_sm)),
+    def set_tiles(self, tx: int, ty: int, zb: int, blocks_per_sm: int = 0, mode: int = 0) -> None:
+        """mode 0: persistent work-list solve with these tiles; mode 1: concurrent
+        per-member tiled launches (the tiles still describe mode 0's work list)."""
+        _check(self.lib.acEnsembleSetTiles(self._h, AcEnsembleTiles(tx, ty, zb, blocks_per_sm,
+                                                                    mode)),
                "acEnsembleSetTiles")
 
     def _cache_key(self) -> str:
@@ -158,7 +163,7 @@ class Ensemble:
         ms = C.c_double()
         _check(self.lib.acEnsembleAutotune(self._h, C.byref(best), C.byref(ms)),
                "acEnsembleAutotune")
-        tiles = (best.tx, best.ty, best.zb, best.blocks_per_sm)
+        tiles = (best.tx, best.ty, best.zb, best.blocks_per_sm, best.mode)
         if use_cache:
             table[key] = list(tiles)
             try:

@@ -465,27 +465,45 @@ def ensemble_leg(args, torch, rank, world):
         e1.synchronize()
         return adist.max_over_ranks(e0.elapsed_time(e1) / k)
 
-    for _ in range(args.warmup):
-        e.integrate_step()
-        e.integrate_step_sequential()
-    e.synchronize()
-    l0 = e.launch_count()
+    # a step is a few ms: time at least 20, with the clock sampler (a
+    # subprocess whose start-up would stall launches) running before warm-up
+    k = max(args.steps, 20)
     with ClockSampler(torch.cuda.current_device()) as clk:
-        ms = timed(e.integrate_step, args.steps)
-    launches = e.launch_count() - l0
+        for _ in range(args.warmup):
+            e.integrate_step()
+        e.synchronize()
+        l0 = e.launch_count()
+        ms = timed(e.integrate_step, k)
+        launches = (e.launch_count() - l0) // k
+    for _ in range(args.warmup):
+        e.integrate_step_sequential()
     l1 = e.launch_count()
-    ms_seq = timed(e.integrate_step_sequential, args.steps)
-    launches_seq = e.launch_count() - l1
+    ms_seq = timed(e.integrate_step_sequential, k)
+    launches_seq = (e.launch_count() - l1) // k
+    # both step modes with the tuned work-list tiles, for the record
+    modes = {}
+    for mode in (0, 1):
+        try:
+            e.set_tiles(*tiles[:4], mode=mode)
+        except Exception:
+            continue
+        for _ in range(args.warmup):
+            e.integrate_step()
+        e.synchronize()
+        modes[mode] = timed(e.integrate_step, k)
+    e.set_tiles(*tiles)
     e.destroy()
     peak, _ = peaks()
     achieved = BYTES_PER_CELL_STEP["fp32comp"] * total_cells / world / (ms * 1e-3) / 1e9
     return {"workload": "64 members, N in {32,48,64,96}, nu/eta log-U[1e-3,1e-2], "
                         "seeds 100..163, FP32 compensated, dt=1e-3",
             "members": len(members), "cells": total_cells, "value": total_cells / (ms * 1e-3),
-            "unit": UNIT, "ms_per_step": ms, "gpu_launches": launches,
+            "unit": UNIT, "ms_per_step": ms, "steps": k, "gpu_launches_per_step": launches,
             "sequential": {"value": total_cells / (ms_seq * 1e-3), "ms_per_step": ms_seq,
-                           "gpu_launches": launches_seq},
+                           "gpu_launches_per_step": launches_seq},
             "speedup_vs_sequential": ms_seq / ms, "tiles": list(tiles),
+            "ms_per_step_by_mode": {"persistent": modes.get(0),
+                                    "tiled_per_member_graph": modes.get(1)},
             "autotune_solve_ms": tune_ms, "clocks": clk.summary(),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak,

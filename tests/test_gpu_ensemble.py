@@ -71,7 +71,7 @@ def test_graph_sequential_and_tiles_agree():
             e.set_timesteps(DT)
             if mode == "tiles":
                 e.set_tiles(16, 8, 5, 1)
-                assert e.tiles == (16, 8, 5, 1)
+                assert e.tiles == (16, 8, 5, 1, 0)
             for _ in range(2):
                 if mode == "sequential":
                     e.integrate_step_sequential()
@@ -92,7 +92,8 @@ def test_autotune_keeps_state_and_results(tmp_path):
         before = [e.store_member(m) for m in range(e.n)]
         tiles, ms = e.autotune(cache=tmp_path / "tiles.json")
         assert ms is not None and ms > 0
-        tx, ty, zb, bps = tiles
+        tx, ty, zb, bps, mode = tiles
+        assert mode in (0, 1)
         assert tx * ty % 32 == 0 and tx * ty <= 256 and zb >= 1
         for m in range(e.n):  # tuning leaves the in-buffers as they were
             assert np.array_equal(e.store_member(m), before[m])
@@ -105,6 +106,43 @@ def test_autotune_keeps_state_and_results(tmp_path):
             assert t2 == tiles and ms2 is None
     for m in range(len(infos)):
         assert np.array_equal(got[m], _device_run(infos[m], seeds[m], 1))
+
+
+def _device_tiled(info, seed, steps):
+    with Device(info) as d:
+        d.load_mesh(seeded_mesh(info, seed))
+        for _ in range(steps):
+            d.integrate_step(DT)
+        d.synchronize()
+        return d.store_mesh()
+
+
+@pytest.mark.parametrize("precision", [1, 0])
+def test_mode1_members_equal_default_device(precision):
+    """Mode 1 runs each member through the kernel its own Device uses (tiled,
+    or plain where the mesh does not fit the tiled kernel, e.g. 32^3 in FP32
+    and nx = 24): the same bits as that Device."""
+    infos, seeds = _members(precision, [32, 48, (40, 36, 44), 64, 96, (24, 32, 16)])
+    with Ensemble(infos) as e:
+        e.load_seeded(seeds)
+        e.set_timesteps(DT)
+        e.set_tiles(32, 4, 8, 0, mode=1)
+        for _ in range(3):
+            e.integrate_step()
+        e.synchronize()
+        got = [e.store_member(m) for m in range(e.n)]
+        # dt changes take effect in mode 1 too (its launches take dt as a parameter)
+        e.set_timesteps(2 * DT)
+        e.integrate_step()
+        e.synchronize()
+        twice = e.store_member(0)
+    for m in range(len(infos)):
+        assert np.array_equal(got[m], _device_tiled(infos[m], seeds[m], 3)), m
+    with Device(infos[0]) as d:
+        d.load_mesh(got[0])
+        d.integrate_step(2 * DT)
+        d.synchronize()
+        assert np.array_equal(twice[:, 3:-3, 3:-3, 3:-3], d.store_mesh()[:, 3:-3, 3:-3, 3:-3])
 
 
 def test_fp64_member_matches_oracle():
