@@ -568,12 +568,12 @@ reduce_member(const Ensemble e, const int m, const AcReduction r, const int kind
 } // namespace
 
 extern "C" AcResult
-acEnsembleCreate(const int device_id, const int n, const AcMeshInfo* configs, Ensemble* out)
+acEnsembleCreate(const int device_id, const int n, const AcMeshInfo* member_infos, Ensemble* out)
 {
     if (!out)
         return AC_FAILURE;
     *out = NULL;
-    if (n < 1 || !configs)
+    if (n < 1 || !member_infos)
         return AC_FAILURE;
     int count = 0;
     AC_CUDA_CHECK(cudaGetDeviceCount(&count));
@@ -594,7 +594,7 @@ acEnsembleCreate(const int device_id, const int n, const AcMeshInfo* configs, En
         }                                                                                     \
     } while (0)
     for (int m = 0; m < n; ++m) {
-        AcMeshInfo info = configs[m];
+        AcMeshInfo info = member_infos[m];
         if (acHostUpdateParams(&info) != AC_SUCCESS) {
             fprintf(stderr, "astaroth_b200: ensemble member %d: invalid AcMeshInfo\n", m);
             destroy(e);

@@ -94,7 +94,7 @@ def mesh_struct(fields: np.ndarray, info: AcMeshInfo) -> AcMesh:
 
 def seeded_mesh(info: AcMeshInfo, seed: int, amp_scalar: float = 1e-5, sigma_uu: float = 1e-3,
                 sigma_aa: float = 1e-4) -> np.ndarray:
-    """Seeded initial condition of the benchmark configs (every cell incl. halos):
+    """Seeded initial condition of the benchmark workloads (every cell incl. halos):
     lnrho, entropy ~ U(-amp, amp); uu ~ N(0, sigma_uu^2); aa ~ N(0, sigma_aa^2)."""
     lib = capi.load()
     f = empty_mesh(info)

@@ -2,7 +2,7 @@
 
 Workload: one RK3 step (3 x [periodic halo fill + substep + swap]) of the
 8-field MHD system at 512^3 interior, FP64, seeded synthetic fields of the
-benchmark configs (lnrho, s ~ U(-1e-5, 1e-5), uu ~ N(0, 1e-3^2),
+benchmark workloads (lnrho, s ~ U(-1e-5, 1e-5), uu ~ N(0, 1e-3^2),
 aa ~ N(0, 1e-4^2)), nu = eta = 5e-3, cs = 1, gamma = 5/3, dt = 1e-3.
 
   python bench.py [--gpus N --steps K --warmup W] [--n 512] [--impl reference]

@@ -6,7 +6,7 @@ the torch.autograd wrapper (astaroth_b200.autograd).
   tests/test_oracle.py);
 * the gradient of J = E_kin + E_mag after several steps w.r.t. the initial
   fields and nu, eta against the same CPU reference gradient;
-* config 4 (64^3, 200 steps, dt = 1e-3, seed 4, checkpoints every 20 steps):
+* 64^3, 200 steps, dt = 1e-3, seed 4, checkpoints every 20 steps:
   central finite differences (h = 1e-6) in 32 random directions and in nu, eta,
   and a dot-product test of the adjoint of the 200-step map.
 """
@@ -127,8 +127,8 @@ def test_tape_sweep_equals_per_substep_sweep():
         assert abs(a - b) <= 1e-12 * abs(b)
 
 
-def test_config4_fd_dot_product_and_cost():
-    """Config 4: 64^3, 200 steps, dt = 1e-3, seed 4, checkpoints every 20 steps."""
+def test_64_cubed_200_steps_fd_dot_product_and_cost():
+    """64^3, 200 steps, dt = 1e-3, seed 4, checkpoints every 20 steps."""
     torch = _torch()
     from astaroth_b200 import autograd as AG
     info = ab.make_info(64, **ab.CONFIG_PARAMS)
@@ -209,7 +209,7 @@ def test_config4_fd_dot_product_and_cost():
                                          device="cuda") * torch.from_numpy(SCALES).cuda()[:, None, None, None])
         lhs = float(((run(f0 + h * d) - run(f0 - h * d)) / (2 * h) * lam)[:, 3:-3, 3:-3, 3:-3].sum())
         rhs = float((x1.grad * d).sum())
-    print(f"\nconfig4: forward {t_fwd * 1e3:.1f} ms, adjoint (recompute + reverse) {t_bwd * 1e3:.1f} ms,"
+    print(f"\nadjoint 64^3 x 200 steps: forward {t_fwd * 1e3:.1f} ms, adjoint (recompute + reverse) {t_bwd * 1e3:.1f} ms,"
           f" ratio {t_bwd / t_fwd:.2f}, peak torch memory {peak / 2**20:.0f} MiB,"
           f" worst FD rel err {worst:.2e} (h=1e-6), {worst_h5:.2e} (h=1e-5)")
     assert worst_floor <= 1e-6

@@ -190,7 +190,7 @@ def test_errors():
         Ensemble([make_info(32, precision=0), make_info(32, precision=1)])
 
 
-def test_config3_ensemble_graph_equals_sequential():
+def test_64_member_ensemble_graph_equals_sequential():
     """The 64-member FP32-compensated ensemble: graph == sequential launches
     after 2 steps; prints both rates."""
     import time
@@ -214,7 +214,7 @@ def test_config3_ensemble_graph_equals_sequential():
                 e.integrate_step() if mode == "graph" else e.integrate_step_sequential()
             e.synchronize()
             rates[mode] = 5 * e.cells / (time.perf_counter() - t0)
-    print(f"config3: {rates['graph']:.3e} cell-updates/s (graph, persistent), "
+    print(f"64-member ensemble: {rates['graph']:.3e} cell-updates/s (graph, persistent), "
           f"{rates['sequential']:.3e} (sequential plain launches)")
     for a, b in zip(*outs):
         assert np.array_equal(a, b)

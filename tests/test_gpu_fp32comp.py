@@ -63,7 +63,7 @@ def test_periodic_bitexact_on_pairs(n):
 
 
 def test_fp32comp_vs_fp64_100_steps():
-    """Config 1 accuracy bar at 128^3: per-field rel L-inf <= 1e-5 after 100 steps."""
+    """Accuracy bar at 128^3: per-field rel L-inf <= 1e-5 after 100 steps."""
     a = run(128, 2, 100, precision=0)
     b = run(128, 2, 100, precision=1)
     err = oracle.rel_linf(b, a)

@@ -123,8 +123,8 @@ def test_integration_vs_reference_golden(name):
     assert e10.max() <= TOL_1STEP * 10, e10
 
 
-def test_config0_128_one_step():
-    """Config 0: 128^3, seed 1, dt = 1e-3, 1 step against the oracle."""
+def test_128_cubed_one_step():
+    """128^3, seed 1, dt = 1e-3: one step against the oracle."""
     info = ab.make_info(128, **ab.CONFIG_PARAMS)
     f = ab.seeded_mesh(info, 1)
     ref = f.copy()
@@ -134,7 +134,7 @@ def test_config0_128_one_step():
     assert err.max() <= TOL_1STEP, err
 
 
-def test_config0_100_steps_32():
+def test_100_steps_32_cubed():
     info = ab.make_info(32, **ab.CONFIG_PARAMS)
     f = ab.seeded_mesh(info, 1)
     ref = f.copy()
@@ -145,8 +145,8 @@ def test_config0_100_steps_32():
 
 
 @pytest.mark.slow
-def test_config0_128_100_steps():
-    """Config 0 in full: 128^3, 100 steps against the oracle (minutes of CPU)."""
+def test_128_cubed_100_steps():
+    """128^3, seed 1, 100 steps against the oracle (minutes of CPU)."""
     info = ab.make_info(128, **ab.CONFIG_PARAMS)
     f = ab.seeded_mesh(info, 1)
     ref = f.copy()
@@ -378,7 +378,7 @@ def test_additive_timestep():
 
 
 def test_adaptive_run_is_stable():
-    """Config 2 in miniature: solenoidal modes, FP32-comp, CFL-adaptive dt."""
+    """The adaptive-CFL run in miniature: solenoidal modes, FP32-comp, dt from the maxima."""
     info = ab.make_info(64, precision=1, **ab.CONFIG_PARAMS)
     f = ab.seeded_mesh(info, 3)
     ab.solenoidal_velocity(f, info, seed=3, nmodes=64, kmax=8, amplitude=1e-2)
