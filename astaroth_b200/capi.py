@@ -42,9 +42,10 @@ class IntParam(enum.IntEnum):
     AC_debug_plain_kernel = 2
     AC_upwind = 3
     AC_lforcing = 4
+    AC_lbfield = 5
 
 
-NUM_INT_PARAMS = 5
+NUM_INT_PARAMS = 6
 
 
 class Int3Param(enum.IntEnum):
@@ -265,6 +266,8 @@ SIGNATURES = {
                                               C.POINTER(AcMeshInfo)]),
     "acHostMeshWriteToFile": (C.c_int, [AcMesh, C.c_size_t]),
     "acHostMeshReadFromFile": (C.c_int, [C.c_size_t, C.POINTER(AcMesh)]),
+    "acDeviceStoreBfield": (C.c_int, [Device_p, C.c_int, C.POINTER(C.c_double),
+                                      C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "acDevicePlaneBytes": (C.c_size_t, [Device_p]),
     "acDevicePackPlanes": (C.c_int, [Device_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "acDeviceUnpackPlanes": (C.c_int, [Device_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),

@@ -194,6 +194,20 @@ stream_ok(const Stream s)
     return (int)s >= 0 && (int)s < NUM_STREAMS;
 }
 
+/* The B arrays of AC_lbfield, allocated (zeroed) when the flag is first set;
+ * never during a stream capture (every caller is outside one). */
+static cudaError_t
+ensure_bfield(Device d)
+{
+    if (!d->config.int_params[AC_lbfield] || d->bfield)
+        return cudaSuccess;
+    const size_t bytes = 3 * (size_t)d->geom.mx * d->geom.my * d->geom.mz * sizeof(double);
+    cudaError_t e      = cudaMalloc((void**)&d->bfield, bytes);
+    if (e != cudaSuccess)
+        return e;
+    return cudaMemset(d->bfield, 0, bytes);
+}
+
 static void
 invalidate_tape_graph(Device d)
 {
@@ -233,6 +247,7 @@ release(Device d)
     cudaFree(d->adj_mu);
     cudaFree(d->adj_pgrad);
     cudaFree(d->adj_tape);
+    cudaFree(d->bfield);
     cudaFreeHost(d->host_result);
     for (int s = 0; s < NUM_STREAMS; ++s)
         if (d->streams[s])
@@ -331,6 +346,7 @@ acDeviceCreate(const int id, const AcMeshInfo device_config, Device* device_hand
     if (d->tmap_ok)
         CREATE_CHECK(ac_solve_tiled_init(precision));
     CREATE_CHECK(cudaMallocHost((void**)&d->host_result, sizeof(double)));
+    CREATE_CHECK(ensure_bfield(d));
     CREATE_CHECK(cudaStreamSynchronize(d->streams[0]));
 #undef CREATE_CHECK
 
@@ -436,6 +452,8 @@ refresh_config(Device d, const AcMeshInfo& info)
     }
     d->config = next;
     invalidate_graphs(d);
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    AC_CUDA_CHECK(ensure_bfield(d));
     return AC_SUCCESS;
 }
 
@@ -688,6 +706,21 @@ launch_substep(Device d, cudaStream_t st, const int step, const double dt,
     if (step == 2)
         forcing_for_launch(d->config, dt, &pc);
     const RkCoef rk = ac_rk_coef(step, dt);
+    if (step == 2 && d->config.int_params[AC_lbfield] && d->bfield) {
+        /* B = curl A of this substep's input (the in-buffer is not written) */
+        const void* a[3];
+        double* b[3];
+        const size_t nm = (size_t)d->geom.mx * d->geom.my * d->geom.mz;
+        for (int c = 0; c < 3; ++c) {
+            const int q = VTXBUF_AX + c;
+            a[c] = d->precision == 0 ? (const void*)arr64(d, d->in_idx[q], q)
+                                     : (const void*)arr_hi(d, d->in_idx[q], q);
+            b[c] = d->bfield + c * nm;
+        }
+        const cudaError_t e = ac_launch_bfield(d->geom, a, b, d->precision, sc, st, launches);
+        if (e != cudaSuccess)
+            return e;
+    }
     const int blk   = in_block_index(d);
     const bool tiled = d->solve_variant == 1 && d->tmap_ok && blk >= 0;
     /* substep 2 also produces the CFL maxima of its input state, as the
@@ -1498,6 +1531,25 @@ acDeviceReadMeshFromDisk(const Device d, const char* dir, const char* label, con
     if (res == AC_SUCCESS)
         res = acDeviceSynchronizeStream(d, STREAM_DEFAULT);
     return res;
+}
+
+extern "C" AcResult
+acDeviceStoreBfield(const Device d, const Stream stream, AcReal* bx, AcReal* by, AcReal* bz)
+{
+    if (!d || !stream_ok(stream) || !bx || !by || !bz)
+        return AC_FAILURE;
+    if (!d->config.int_params[AC_lbfield] || !d->bfield) {
+        fprintf(stderr, "astaroth_b200: acDeviceStoreBfield needs AC_lbfield\n");
+        return AC_FAILURE;
+    }
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    const size_t nm = (size_t)d->geom.mx * d->geom.my * d->geom.mz;
+    AcReal* out[3]  = {bx, by, bz};
+    for (int c = 0; c < 3; ++c)
+        AC_CUDA_CHECK(cudaMemcpyAsync(out[c], d->bfield + c * nm, nm * sizeof(double),
+                                      cudaMemcpyDeviceToHost, d->streams[stream]));
+    AC_CUDA_CHECK(cudaStreamSynchronize(d->streams[stream]));
+    return AC_SUCCESS;
 }
 
 extern "C" void*

@@ -109,6 +109,7 @@ static const ParamName param_names[] = {
     {"AC_additive_timestep", 0, AC_additive_timestep},
     {"AC_upwind", 0, AC_upwind},
     {"AC_lforcing", 0, AC_lforcing},
+    {"AC_lbfield", 0, AC_lbfield},
     {"AC_ngrid", 1, AC_ngrid},
     {"AC_nlocal", 1, AC_nlocal},
     {"AC_nu_visc", 2, AC_nu_visc},

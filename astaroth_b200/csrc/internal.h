@@ -171,6 +171,7 @@ struct device_s {
     double* adj_lw;      /* 8 fields */
     double* adj_mu;      /* AC_MU_COUNT fields */
     double* adj_pgrad;   /* 2 values: d/d nu, d/d eta */
+    double* bfield;      /* AC_lbfield: B = curl A, 3 arrays of mx*my*mz doubles */
     double* adj_tape;    /* substep input states of a recomputed segment, 8 fields each */
     int adj_tape_states; /* states the tape holds */
     /* graph of the last acDeviceAdjointTapeForward (steps, dt, in-block, stream) */
@@ -238,6 +239,12 @@ cudaError_t ac_launch_solve_tiled32(const Geom& g, const void* tmap_in, const Fi
 cudaError_t ac_launch_forcing(const Geom& g, void* const* u, float* const* lo, const int precision,
                               const PhysConst& pc, cudaStream_t stream,
                               unsigned long long* launches);
+
+/* B = curl A of the A arrays a[3] (in-buffer, element type of the precision)
+ * into the double arrays b[3] in the host layout (bfield.cu). */
+cudaError_t ac_launch_bfield(const Geom& g, const void* const* a, double* const* b,
+                             const int precision, const StencilCoef& sc, cudaStream_t stream,
+                             unsigned long long* launches);
 
 /* CFL maxima of the in-buffer (cfl.cu); zeroes the three words first. */
 template <typename T>
