@@ -185,6 +185,14 @@ def cpu_reference_sample(n: int, steps: int = 1):
 
 # ---------------------------------------------------------------- reference arm
 
+def workload_config(n: int, world: int) -> dict:
+    """The `config` of both arms' lines."""
+    return {"workload": f"MHD RK3 step, {n}^3 interior + 3-cell halos, 8 fields, FP64, "
+                        f"periodic, dt=1e-3",
+            "n": n, "parallelism": f"replicas x{world}",
+            "l2": f"state {2 * 8 * (n + 6) ** 3 * 8 / 1e9:.1f} GB > 126 MB L2; no flush needed"}
+
+
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
@@ -204,9 +212,7 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f80",
         "data": "synthetic",
-        "config": {"workload": f"MHD RK3 step, {args.n}^3 interior, FP64 state "
-                               f"(CPU sample {REF_SAMPLE_N}^3 per step)",
-                   "n": args.n, "sample_n": REF_SAMPLE_N},
+        "config": dict(workload_config(args.n, world), cpu_sample_n=REF_SAMPLE_N),
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": s["cores"], "kind": s["kind"],
                          "sample": s["sample"]},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -335,10 +341,7 @@ def run_gpu(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded: lnrho,s ~ U(-1e-5,1e-5); uu ~ N(0,1e-3^2); "
                     "aa ~ N(0,1e-4^2))",
-            "config": {"workload": f"MHD RK3 step, {n}^3 interior + 3-cell halos, 8 fields, "
-                                   f"FP64, periodic, dt=1e-3",
-                       "n": n, "parallelism": f"replicas x{world}",
-                       "l2": "state 17.8 GB > 126 MB L2; no flush needed"},
+            "config": workload_config(n, world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "solve (3 launches per RK3 step)",
