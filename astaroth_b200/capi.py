@@ -127,6 +127,17 @@ class MapKernel(enum.IntEnum):
     AC_MAP_VTXBUF3_EXP_SQUARE = 6
     AC_MAP_VTXBUF4_ALFVEN_NORM = 7
     AC_MAP_VTXBUF4_ALFVEN_SQUARE = 8
+    AC_KERNEL_SOLVE = 9
+    AC_KERNEL_CALC_TIMESTEP = 10
+
+
+class RealOutputParam(enum.IntEnum):
+    UU_MAX_ADVEC = 0
+    ALFVEN_SPEED_MAX = 1
+    AC_dt_min = 2
+
+
+NUM_REAL_OUTPUTS = 3
 
 
 AC_SUCCESS, AC_FAILURE, AC_NOT_ALLOCATED = 0, 1, 2
@@ -253,6 +264,12 @@ SIGNATURES = {
     "acDeviceGetTimestepMaxima": (C.c_int, [Device_p, C.POINTER(C.c_double),
                                             C.POINTER(C.c_double)]),
     "acDeviceGetTimestep": (C.c_int, [Device_p, C.POINTER(C.c_double)]),
+    "acDeviceFinishReduceReal": (C.c_int, [Device_p, C.c_int, C.POINTER(C.c_double), C.c_int,
+                                           C.c_int, C.c_int]),
+    "acDeviceFinishReduceRealStream": (C.c_int, [Device_p, C.c_void_p, C.POINTER(C.c_double),
+                                                 C.c_int, C.c_int, C.c_int]),
+    "acDeviceGetOutput": (C.c_double, [Device_p, C.c_int]),
+    "acDeviceSetOutput": (C.c_int, [Device_p, C.c_int, C.c_double]),
     "acDeviceLoadMeshDevice": (C.c_int, [Device_p, C.c_int, C.POINTER(C.c_void_p)]),
     "acDeviceStoreMeshDevice": (C.c_int, [Device_p, C.c_int, C.POINTER(C.c_void_p)]),
     "acDeviceLoadAdjoint": (C.c_int, [Device_p, C.c_int, C.POINTER(C.c_void_p)]),

@@ -792,6 +792,8 @@ acDeviceIntegrateSubstep(const Device d, const Stream stream, const int step_num
     }
     AC_CUDA_CHECK(cudaSetDevice(d->id));
     AC_CUDA_CHECK(launch_substep(d, d->streams[stream], step_number, dt, &d->launches));
+    if (step_number == 2)
+        d->out_set = 0;
     return AC_SUCCESS;
 }
 
@@ -846,6 +848,7 @@ acDeviceIntegrateStep(const Device d, const Stream stream, const AcReal dt)
     const int parity = in_block_index(d);
     if (parity < 0) {
         AC_CUDA_CHECK(record_step(d, st, dt, &d->launches));
+        d->out_set = 0;
         return AC_SUCCESS;
     }
     StepGraph& sg = d->graphs[stream][parity];
@@ -868,6 +871,7 @@ acDeviceIntegrateStep(const Device d, const Stream stream, const AcReal dt)
     }
     AC_CUDA_CHECK(cudaGraphLaunch(sg.exec, st));
     d->launches += 6;
+    d->out_set = 0;
     acDeviceSwapBuffers(d);
     return AC_SUCCESS;
 }
@@ -1035,7 +1039,70 @@ acDeviceCalcTimestep(const Device d, const Stream stream)
     else
         AC_CUDA_CHECK(ac_launch_cfl<float>(d->geom, fields32(d), sc, cs2, d->cfl,
                                            d->streams[stream], &d->launches));
+    d->out_set = 0;
     return AC_SUCCESS;
+}
+
+/* dt of the additive form, mhdsolver.ac:558-569: the minimum over cells of
+ * min(visc_dt, advec_dt); visc_dt is uniform, so the minimum of advec_dt comes
+ * from the maximum of |u| + sqrt(cs^2 + vA^2) */
+static double
+additive_dt(const AcMeshInfo& c, const double advec_sum_max)
+{
+    const double dsmin   = c.real_params[AC_dsmin];
+    double visc          = c.real_params[AC_nu_visc] > c.real_params[AC_eta]
+                               ? c.real_params[AC_nu_visc]
+                               : c.real_params[AC_eta];
+    const double gchi    = c.real_params[AC_gamma] * c.real_params[AC_chi];
+    visc                 = visc > gchi ? visc : gchi;
+    const double visc_dt = visc > 0 ? c.real_params[AC_cdtv] * dsmin * dsmin / visc : INFINITY;
+    const double advec_dt = c.real_params[AC_cdt] * dsmin / advec_sum_max;
+    return visc_dt < advec_dt ? visc_dt : advec_dt;
+}
+
+/* The outputs as the device reduced them, after waiting for `st` (all of the
+ * device's streams when st is NULL). */
+static cudaError_t
+device_outputs(Device d, const cudaStream_t* st, double v[NUM_REAL_OUTPUTS])
+{
+    cudaError_t e = cudaSetDevice(d->id);
+    if (e != cudaSuccess)
+        return e;
+    if (st) {
+        e = cudaStreamSynchronize(*st);
+        if (e != cudaSuccess)
+            return e;
+    }
+    else {
+        for (int s = 0; s < NUM_STREAMS; ++s)
+            if ((e = cudaStreamSynchronize(d->streams[s])) != cudaSuccess)
+                return e;
+    }
+    unsigned long long w[3];
+    if ((e = cudaMemcpy(w, d->cfl, sizeof(w), cudaMemcpyDeviceToHost)) != cudaSuccess)
+        return e;
+    double m[3];
+    memcpy(m, w, sizeof(m));
+    v[UU_MAX_ADVEC]     = m[0];
+    v[ALFVEN_SPEED_MAX] = m[1];
+    v[AC_dt_min]        = additive_dt(d->config, m[2]);
+    return cudaSuccess;
+}
+
+/* The device's outputs with the acDeviceSetOutput values in their place. */
+static cudaError_t
+current_outputs(Device d, double v[NUM_REAL_OUTPUTS])
+{
+    const unsigned all = (1u << NUM_REAL_OUTPUTS) - 1;
+    if ((d->out_set & all) != all) {
+        const cudaError_t e = device_outputs(d, NULL, v);
+        if (e != cudaSuccess)
+            return e;
+    }
+    for (int p = 0; p < NUM_REAL_OUTPUTS; ++p)
+        if (d->out_set >> p & 1)
+            v[p] = d->outputs[p];
+    return cudaSuccess;
 }
 
 extern "C" AcResult
@@ -1043,15 +1110,10 @@ acDeviceGetTimestepMaxima(const Device d, AcReal* uu_max, AcReal* alfven_max)
 {
     if (!d || !uu_max || !alfven_max)
         return AC_FAILURE;
-    AC_CUDA_CHECK(cudaSetDevice(d->id));
-    for (int s = 0; s < NUM_STREAMS; ++s)
-        AC_CUDA_CHECK(cudaStreamSynchronize(d->streams[s]));
-    unsigned long long w[3];
-    AC_CUDA_CHECK(cudaMemcpy(w, d->cfl, sizeof(w), cudaMemcpyDeviceToHost));
-    double v[3];
-    memcpy(v, w, sizeof(v));
-    *uu_max     = v[0];
-    *alfven_max = v[1];
+    double v[NUM_REAL_OUTPUTS];
+    AC_CUDA_CHECK(current_outputs(d, v));
+    *uu_max     = v[UU_MAX_ADVEC];
+    *alfven_max = v[ALFVEN_SPEED_MAX];
     return AC_SUCCESS;
 }
 
@@ -1060,31 +1122,68 @@ acDeviceGetTimestep(const Device d, AcReal* dt)
 {
     if (!d || !dt)
         return AC_FAILURE;
-    AC_CUDA_CHECK(cudaSetDevice(d->id));
-    for (int s = 0; s < NUM_STREAMS; ++s)
-        AC_CUDA_CHECK(cudaStreamSynchronize(d->streams[s]));
-    unsigned long long w[3];
-    AC_CUDA_CHECK(cudaMemcpy(w, d->cfl, sizeof(w), cudaMemcpyDeviceToHost));
-    double v[3];
-    memcpy(v, w, sizeof(v));
-    if (d->config.int_params[AC_additive_timestep]) {
-        /* mhdsolver.ac:558-569: min over cells of min(visc_dt, advec_dt); visc_dt is
-         * uniform, so the minimum of advec_dt comes from the maximum of
-         * |u| + sqrt(cs^2 + vA^2) */
-        const AcMeshInfo& c = d->config;
-        const double dsmin  = c.real_params[AC_dsmin];
-        double visc         = c.real_params[AC_nu_visc] > c.real_params[AC_eta]
-                                  ? c.real_params[AC_nu_visc]
-                                  : c.real_params[AC_eta];
-        const double gchi   = c.real_params[AC_gamma] * c.real_params[AC_chi];
-        visc                = visc > gchi ? visc : gchi;
-        const double visc_dt  = visc > 0 ? c.real_params[AC_cdtv] * dsmin * dsmin / visc : INFINITY;
-        const double advec_dt = c.real_params[AC_cdt] * dsmin / v[2];
-        *dt                   = visc_dt < advec_dt ? visc_dt : advec_dt;
-    }
-    else {
-        *dt = acHostTimestepFromMaxima(d->config, v[0], v[1]);
-    }
+    double v[NUM_REAL_OUTPUTS];
+    AC_CUDA_CHECK(current_outputs(d, v));
+    *dt = d->config.int_params[AC_additive_timestep]
+              ? v[AC_dt_min]
+              : acHostTimestepFromMaxima(d->config, v[UU_MAX_ADVEC], v[ALFVEN_SPEED_MAX]);
+    return AC_SUCCESS;
+}
+
+static AcResult
+finish_reduce(Device d, const cudaStream_t st, AcReal* result, const AcKernel kernel,
+              const AcReduceOp op, const AcRealOutputParam output)
+{
+    if (!d || !result || (int)output < 0 || output >= NUM_REAL_OUTPUTS ||
+        (kernel != AC_KERNEL_SOLVE && kernel != AC_KERNEL_CALC_TIMESTEP))
+        return AC_FAILURE;
+    const AcReduceOp own = output == AC_dt_min ? AC_REDUCE_OP_MIN : AC_REDUCE_OP_MAX;
+    if (op != own)
+        return AC_FAILURE;
+    double v[NUM_REAL_OUTPUTS];
+    AC_CUDA_CHECK(device_outputs(d, &st, v));
+    d->out_set &= ~(1u << output);
+    *result = v[output];
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceFinishReduceReal(Device d, const Stream stream, AcReal* result, const AcKernel kernel,
+                         const AcReduceOp reduce_op, const AcRealOutputParam output)
+{
+    if (!d || !stream_ok(stream))
+        return AC_FAILURE;
+    return finish_reduce(d, d->streams[stream], result, kernel, reduce_op, output);
+}
+
+extern "C" AcResult
+acDeviceFinishReduceRealStream(Device d, struct CUstream_st* stream, AcReal* result,
+                               const AcKernel kernel, const AcReduceOp reduce_op,
+                               const AcRealOutputParam output)
+{
+    return finish_reduce(d, (cudaStream_t)stream, result, kernel, reduce_op, output);
+}
+
+extern "C" AcReal
+acDeviceGetOutput(const Device d, const AcRealOutputParam param)
+{
+    if (!d || (int)param < 0 || param >= NUM_REAL_OUTPUTS)
+        return NAN;
+    if (d->out_set >> param & 1)
+        return d->outputs[param];
+    double v[NUM_REAL_OUTPUTS];
+    if (device_outputs(d, NULL, v) != cudaSuccess)
+        return NAN;
+    return v[param];
+}
+
+extern "C" AcResult
+acDeviceSetOutput(const Device d, const AcRealOutputParam param, const AcReal value)
+{
+    if (!d || (int)param < 0 || param >= NUM_REAL_OUTPUTS)
+        return AC_FAILURE;
+    d->outputs[param] = value;
+    d->out_set |= 1u << param;
     return AC_SUCCESS;
 }
 
@@ -1311,6 +1410,7 @@ acDeviceAdjointTapeForward(const Device d, const Stream stream, const int steps,
     }
     AC_CUDA_CHECK(cudaGraphLaunch(d->tape_exec, st));
     d->launches += 9ull * steps;
+    d->out_set = 0;
     if ((3 * steps) & 1) /* three swaps per step */
         acDeviceSwapBuffers(d);
     return AC_SUCCESS;

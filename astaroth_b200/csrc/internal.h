@@ -178,6 +178,10 @@ struct device_s {
     cudaGraphExec_t tape_exec;
     int tape_valid, tape_steps, tape_blk, tape_stream;
     double tape_dt;
+    /* acDeviceSetOutput values; bit p of out_set says output p holds one, until
+     * the next launch that recomputes the CFL words */
+    double outputs[NUM_REAL_OUTPUTS];
+    unsigned out_set;
     unsigned long long launches;
 };
 

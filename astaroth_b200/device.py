@@ -244,6 +244,21 @@ class Device:
         _check(self.lib.acDeviceGetTimestep(self._h, C.byref(dt)), "acDeviceGetTimestep")
         return dt.value
 
+    def finish_reduce(self, output, kernel=capi.MapKernel.AC_KERNEL_SOLVE, stream: int = 0) -> float:
+        """acDeviceFinishReduceReal of one CFL output (capi.RealOutputParam)."""
+        op = (capi.ReduceOp.AC_REDUCE_OP_MIN if output == capi.RealOutputParam.AC_dt_min
+              else capi.ReduceOp.AC_REDUCE_OP_MAX)
+        r = C.c_double()
+        _check(self.lib.acDeviceFinishReduceReal(self._h, stream, C.byref(r), kernel, op, output),
+               "acDeviceFinishReduceReal")
+        return r.value
+
+    def get_output(self, output) -> float:
+        return self.lib.acDeviceGetOutput(self._h, output)
+
+    def set_output(self, output, value: float) -> None:
+        _check(self.lib.acDeviceSetOutput(self._h, output, value), "acDeviceSetOutput")
+
     # ---- caller-owned device arrays (torch tensors of shape (8, mz, my, mx), float64) ----
     @staticmethod
     def _ptrs(t):

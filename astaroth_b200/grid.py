@@ -250,12 +250,19 @@ class Grid:
             d.calc_timestep()
 
     def timestep(self) -> float:
-        """dt from the CFL maxima of all slabs (the last substep 2, or
-        calc_timestep), combined with max as the reference's allreduce."""
-        us, vs = zip(*(d.timestep_maxima() for d in self.devs))
-        u = self.transport.combine([max(us)], "max")
-        va = self.transport.combine([max(vs)], "max")
-        return self.lib.acHostTimestepFromMaxima(self.info, u, va)
+        """dt from the CFL outputs of all slabs (the last substep 2, or
+        calc_timestep): each output finished on every slab, combined with its
+        own operation (max, or min for AC_dt_min) and set back on the slabs,
+        as acGridFinalizeReduce (src/core/grid.cc:3004-3024); then the dt of
+        the maximum or the additive form (AC_additive_timestep)."""
+        out = capi.RealOutputParam
+        for p, op in ((out.UU_MAX_ADVEC, "max"), (out.ALFVEN_SPEED_MAX, "max"),
+                      (out.AC_dt_min, "min")):
+            vals = [d.finish_reduce(p) for d in self.devs]
+            v = self.transport.combine([{"max": max, "min": min}[op](vals)], op)
+            for d in self.devs:
+                d.set_output(p, v)
+        return self.devs[0].timestep()
 
 
 __all__ = ["Grid", "LocalTransport", "DistTransport", "decompose", "slab_info"]

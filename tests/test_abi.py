@@ -39,7 +39,7 @@ def header_enum_values():
                 continue
             if "=" in item:
                 name, v = (s.strip() for s in item.split("="))
-                cur = int(v)
+                cur = vals[v] if v in vals else int(v)
             else:
                 name, cur = item, cur + 1
             vals[name] = cur
@@ -69,6 +69,9 @@ def test_python_enums_match_header():
         assert v[e.name] == e.value
     for e in capi.ReduceOp:
         assert v[e.name] == e.value
+    for e in capi.RealOutputParam:
+        assert v[e.name] == e.value
+    assert v["NUM_REAL_OUTPUTS"] == capi.NUM_REAL_OUTPUTS == len(capi.RealOutputParam)
     assert v["STREAM_ALL"] == capi.STREAM_ALL
 
 
