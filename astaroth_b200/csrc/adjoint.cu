@@ -26,10 +26,12 @@
 
 namespace {
 
-/* z planes per thread of the gather: consecutive planes of one column share
- * most stencil taps, which then come from L1.  (The local kernel keeps one
- * plane per thread: a loop there spills its 254 registers.) */
-constexpr int KZ = 4;
+/* z planes per thread of the gather.  Consecutive planes of one column share
+ * most stencil taps through L1, but the kernel is latency-bound, and one plane
+ * per thread (8x the blocks) measured 10% faster per adjoint substep at 64^3
+ * than 2, 4 or 8 planes.  (The local kernel also keeps one plane per thread:
+ * a loop there spills its 254 registers.) */
+constexpr int KZ = 1;
 
 __global__ void __launch_bounds__(128)
 adj_local_kernel(const Geom g, const AdjointFields a, const StencilCoef sc, const PhysConst pc,
