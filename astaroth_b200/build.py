@@ -32,7 +32,7 @@ CU_SOURCES = ["device.cu", "solve.cu", "solve_tiled.cu", "boundconds.cu", "reduc
               "adjoint.cu", "ensemble.cu", "forcing.cu", "bfield.cu"]
 C_SOURCES = ["host.c"]
 HEADERS = ["internal.h", "mhd_rhs.cuh", "mhd_rhs_adjoint.cuh", "stencil_plain.cuh", "solve_cell.cuh",
-           "halo.cuh"]
+           "halo.cuh", "tma_ring.cuh"]
 
 
 def _nvcc() -> str:

@@ -32,8 +32,11 @@
 
 #include "internal.h"
 #include "mhd_rhs.cuh"
+#include "tma_ring.cuh"
 
 namespace {
+
+using namespace tma_ring;
 
 constexpr int TX     = 32;
 constexpr int TY     = 4;
@@ -42,9 +45,6 @@ constexpr int RING   = 8;
 constexpr int ZCHUNK = 64;
 constexpr int NCELL  = TX * TY; /* cells per tile, one per thread of a group */
 constexpr int XCHG   = (AC_H2M_COUNT + AC_M2H_COUNT) * NCELL; /* exchange entries */
-/* try_wait may suspend the thread for a short, implementation-defined time per
- * call; 2^22 calls bound a wait to seconds even if a copy never lands. */
-constexpr long long kWaitLimit = 1LL << 22;
 
 template <typename T>
 struct Tile;
@@ -52,13 +52,11 @@ template <>
 struct Tile<double> {
     static constexpr int HXP  = TX + 2 * NGHOST; /* 38 x 8 B = 304 B rows */
     static constexpr int MINB = 1;
-    static constexpr CUtensorMapDataType kType = CU_TENSOR_MAP_DATA_TYPE_FLOAT64;
 };
 template <>
 struct Tile<float> {
     static constexpr int HXP  = 40; /* 38 rounded up: 160 B rows */
     static constexpr int MINB = 2;
-    static constexpr CUtensorMapDataType kType = CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
 };
 
 template <typename T>
@@ -70,65 +68,6 @@ struct Layout {
     static constexpr size_t SMEM_BYTES   = (size_t)RING * SLOT_BYTES + (size_t)XCHG * sizeof(T) +
                                          RING * sizeof(uint64_t);
 };
-
-__device__ __forceinline__ uint32_t
-smem_addr(const void* p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ void
-mbar_init(uint64_t* bar, const unsigned count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count)
-                 : "memory");
-}
-
-__device__ __forceinline__ void
-fence_barrier_init()
-{
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-
-__device__ __forceinline__ void
-mbar_arrive_expect_tx(uint64_t* bar, const unsigned bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool
-mbar_try_wait(uint64_t* bar, const unsigned parity)
-{
-    uint32_t ok;
-    asm volatile("{\n\t.reg .pred p;\n\t"
-                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                 "selp.u32 %0, 1, 0, p;\n\t}"
-                 : "=r"(ok)
-                 : "r"(smem_addr(bar)), "r"(parity)
-                 : "memory");
-    return ok != 0;
-}
-
-__device__ __forceinline__ bool
-mbar_wait_bounded(uint64_t* bar, const unsigned parity)
-{
-    for (long long it = 0; it < kWaitLimit; ++it)
-        if (mbar_try_wait(bar, parity))
-            return true;
-    return false;
-}
-
-__device__ __forceinline__ void
-tma_load_plane(void* dst, const CUtensorMap* map, uint64_t* bar, const int x, const int y,
-               const int z)
-{
-    asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-                 " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(smem_addr(dst)),
-                 "l"(map), "r"(x), "r"(y), "r"(z), "r"(0), "r"(smem_addr(bar))
-                 : "memory");
-}
 
 /* Taps of field q at offset (dx, dy, dz) from this thread's cell. */
 template <typename T>
@@ -457,25 +396,6 @@ encode_fn()
     return fn;
 }
 
-template <typename T>
-bool
-make_map(void* map_out, void* base, const Geom& g)
-{
-    EncodeTiledFn fn = encode_fn();
-    if (!fn)
-        return false;
-    const cuuint64_t dims[4]    = {(cuuint64_t)g.mx, (cuuint64_t)g.my, (cuuint64_t)g.mz,
-                                   (cuuint64_t)AC_NF};
-    const cuuint64_t strides[3] = {(cuuint64_t)g.px * sizeof(T), (cuuint64_t)g.pxy * sizeof(T),
-                                   (cuuint64_t)g.cells * sizeof(T)};
-    const cuuint32_t box[4]     = {(cuuint32_t)Tile<T>::HXP, HY, 1, AC_NF};
-    const cuuint32_t estr[4]    = {1, 1, 1, 1};
-    const CUresult r = fn((CUtensorMap*)map_out, Tile<T>::kType, 4, base, dims, strides, box, estr,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS;
-}
-
 /* Planes per CTA: ZCHUNK, halved (down to 8) while the grid would have fewer
  * than two CTAs per SM of the 148.  Every chunk reads 6 halo planes beyond its
  * own, so long chunks are cheaper where the grid is large enough. */
@@ -523,11 +443,35 @@ ac_tiled_supported(const Geom& g, const int precision)
 }
 
 bool
+ac_encode_field_map(void* map_out, void* base, const Geom& g, const int precision,
+                    const unsigned box_x, const unsigned box_y)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn)
+        return false;
+    const size_t esz            = precision == 0 ? sizeof(double) : sizeof(float);
+    const cuuint64_t dims[4]    = {(cuuint64_t)g.mx, (cuuint64_t)g.my, (cuuint64_t)g.mz,
+                                   (cuuint64_t)AC_NF};
+    const cuuint64_t strides[3] = {(cuuint64_t)g.px * esz, (cuuint64_t)g.pxy * esz,
+                                   (cuuint64_t)g.cells * esz};
+    const cuuint32_t box[4]     = {box_x, box_y, 1, AC_NF};
+    const cuuint32_t estr[4]    = {1, 1, 1, 1};
+    const CUresult r =
+        fn((CUtensorMap*)map_out,
+           precision == 0 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4,
+           base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+bool
 ac_make_tensor_map(void* map_out, void* base, const Geom& g, const int precision)
 {
     if (!ac_tiled_supported(g, precision))
         return false;
-    return precision == 0 ? make_map<double>(map_out, base, g) : make_map<float>(map_out, base, g);
+    const unsigned hxp = precision == 0 ? Tile<double>::HXP : Tile<float>::HXP;
+    return ac_encode_field_map(map_out, base, g, precision, hxp, HY);
 }
 
 /* Opts the kernel in to its dynamic shared memory on the current device; called

@@ -418,7 +418,7 @@ def fp32comp_leg(args, ab, torch, host, dev64, info64):
         shape = ab.empty_mesh(info64).shape[1:]
         fa = np.zeros(shape)
         fb = np.zeros(shape)
-        errs = []
+        errs, errs2 = [], []
         for q in range(8):
             # one field at a time: an AcMesh whose only buffer is field q
             sa, sb = ab.capi.AcMesh(), ab.capi.AcMesh()
@@ -431,8 +431,12 @@ def fp32comp_leg(args, ab, torch, host, dev64, info64):
             ib = fb[3:-3, 3:-3, 3:-3]
             den = float(np.abs(ia).max()) or 1.0
             errs.append(float(np.abs(ib - ia).max()) / den)
+            den2 = float(np.sqrt(np.sum(ia * ia))) or 1.0
+            errs2.append(float(np.sqrt(np.sum((ib - ia) ** 2))) / den2)
         out["rel_linf_vs_fp64"] = {"steps": args.accuracy_steps, "per_field": errs,
                                    "max": max(errs)}
+        out["rel_l2_vs_fp64"] = {"steps": args.accuracy_steps, "per_field": errs2,
+                                 "max": max(errs2)}
     dev.destroy()
     return out
 
