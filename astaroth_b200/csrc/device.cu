@@ -538,6 +538,16 @@ host_matches(const Device d, const AcMeshInfo& host)
     return m.x == d->geom.mx && m.y == d->geom.my && m.z == d->geom.mz;
 }
 
+/* The result of a whole-mesh transfer from its per-field results: AC_FAILURE
+ * if any field failed, else AC_NOT_ALLOCATED if any host field was NULL. */
+static AcResult
+worst(const AcResult a, const AcResult b)
+{
+    if (a == AC_FAILURE || b == AC_FAILURE)
+        return AC_FAILURE;
+    return a == AC_NOT_ALLOCATED || b == AC_NOT_ALLOCATED ? AC_NOT_ALLOCATED : AC_SUCCESS;
+}
+
 extern "C" AcResult
 acDeviceLoadVertexBuffer(const Device d, const Stream stream, const AcMesh host_mesh,
                          const VertexBufferHandle h)
@@ -573,10 +583,10 @@ acDeviceLoadVertexBuffer(const Device d, const Stream stream, const AcMesh host_
 extern "C" AcResult
 acDeviceLoadMesh(const Device d, const Stream stream, const AcMesh host_mesh)
 {
-    int res = 0;
+    AcResult res = AC_SUCCESS;
     for (int q = 0; q < AC_NF; ++q)
-        res |= acDeviceLoadVertexBuffer(d, stream, host_mesh, (VertexBufferHandle)q);
-    return (AcResult)res;
+        res = worst(res, acDeviceLoadVertexBuffer(d, stream, host_mesh, (VertexBufferHandle)q));
+    return res;
 }
 
 extern "C" AcResult
@@ -613,10 +623,10 @@ acDeviceStoreVertexBuffer(const Device d, const Stream stream, const VertexBuffe
 extern "C" AcResult
 acDeviceStoreMesh(const Device d, const Stream stream, AcMesh* host_mesh)
 {
-    int res = 0;
+    AcResult res = AC_SUCCESS;
     for (int q = 0; q < AC_NF; ++q)
-        res |= acDeviceStoreVertexBuffer(d, stream, (VertexBufferHandle)q, host_mesh);
-    return (AcResult)res;
+        res = worst(res, acDeviceStoreVertexBuffer(d, stream, (VertexBufferHandle)q, host_mesh));
+    return res;
 }
 
 extern "C" AcResult

@@ -302,6 +302,22 @@ def test_api_errors_and_state():
         dev.periodic_boundconds()
         dev.synchronize()
         assert dev.launch_count() > 0
+        # a dead (NULL) host field: AC_NOT_ALLOCATED, the other fields still move
+        # (the reference's acDeviceLoadMesh / acDeviceStoreMesh, device.cc:671-672)
+        g = ab.seeded_mesh(info, 2)
+        m = ab.device.mesh_struct(g, info)
+        m.vertex_buffer[5] = None
+        assert lib.acDeviceLoadMesh(dev.handle, 0, m) == capi.AC_NOT_ALLOCATED
+        dev.synchronize()
+        out = dev.store_mesh()
+        assert np.array_equal(out[4], g[4]) and np.array_equal(out[6], g[6])
+        assert not np.array_equal(out[5], g[5])
+        back = np.zeros_like(g)
+        mb = ab.device.mesh_struct(back, info)
+        mb.vertex_buffer[2] = None
+        assert lib.acDeviceStoreMesh(dev.handle, 0, capi.C.byref(mb)) == capi.AC_NOT_ALLOCATED
+        dev.synchronize()
+        assert np.array_equal(back[3], out[3]) and not back[2].any()
     assert lib.acDeviceSynchronizeStream(None, 0) == 1
 
 
