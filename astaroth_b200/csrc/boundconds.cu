@@ -124,6 +124,30 @@ join_kernel(const Geom g, const float* __restrict__ hi, const float* __restrict_
     }
 }
 
+/* Plane ranges of up to 16 arrays to or from one contiguous buffer, in 8-byte
+ * words: word w of array a is arrays[a][offset + w] and buffer[a * count + w]
+ * (pack) or the reverse (unpack); grid-stride over all arrays' words. */
+struct PlaneArrays {
+    unsigned long long* a[2 * AC_NF];
+};
+
+__global__ void
+planes_kernel(const PlaneArrays arr, const int narrays, const long long offset,
+              const long long count, unsigned long long* __restrict__ buffer, const bool pack)
+{
+    const long long total = (long long)narrays * count;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int a         = (int)(t / count);
+        const long long w   = t - (long long)a * count;
+        unsigned long long* f = arr.a[a] + offset + w;
+        if (pack)
+            buffer[t] = *f;
+        else
+            *f = buffer[t];
+    }
+}
+
 /* dst = src for n2 double2 pairs (both 16-byte aligned), grid-stride */
 __global__ void
 copy2_kernel(const double2* __restrict__ src, double2* __restrict__ dst, const long long n2)
@@ -225,6 +249,28 @@ ac_launch_copy(const double* src, double* dst, const long long count, cudaStream
                                stream);
     copy2_kernel<<<grid_for(count / 2, 256), 256, 0, stream>>>((const double2*)src,
                                                               (double2*)dst, count / 2);
+    if (launches)
+        ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t
+ac_launch_planes(void* const* arrays, const int narrays, const long long offset_bytes,
+                 const long long bytes, void* buffer, const bool pack, cudaStream_t stream,
+                 unsigned long long* launches)
+{
+    if (narrays < 1 || narrays > 2 * AC_NF || (offset_bytes & 7) || (bytes & 7) ||
+        ((uintptr_t)buffer & 7))
+        return cudaErrorInvalidValue;
+    PlaneArrays arr;
+    for (int a = 0; a < narrays; ++a) {
+        if ((uintptr_t)arrays[a] & 7)
+            return cudaErrorInvalidValue;
+        arr.a[a] = (unsigned long long*)arrays[a];
+    }
+    const long long count = bytes / 8;
+    planes_kernel<<<grid_for((long long)narrays * count, 256), 256, 0, stream>>>(
+        arr, narrays, offset_bytes / 8, count, (unsigned long long*)buffer, pack);
     if (launches)
         ++*launches;
     return cudaGetLastError();

@@ -1492,17 +1492,17 @@ copy_planes(const Device d, const Stream stream, const int z0, const int nplanes
     if (!planes_ok(d, z0, nplanes) || !buffer || !stream_ok(stream))
         return AC_FAILURE;
     AC_CUDA_CHECK(cudaSetDevice(d->id));
-    const size_t es    = elem_size(d);
-    const size_t bytes = (size_t)nplanes * d->geom.pxy * es;
+    const size_t es = elem_size(d);
+    void* arrays[2 * AC_NF];
     for (int a = 0; a < plane_arrays(d); ++a) {
         const int q = a % AC_NF;
-        char* arr   = a < AC_NF ? (char*)d->hi[d->in_idx[q]] + (size_t)q * d->geom.cells * es
-                                : (char*)arr_lo(d, d->in_idx[q], q);
-        char* field = arr + (size_t)z0 * d->geom.pxy * es;
-        char* buf   = buffer + (size_t)a * bytes;
-        AC_CUDA_CHECK(cudaMemcpyAsync(pack ? buf : field, pack ? field : buf, bytes,
-                                      cudaMemcpyDeviceToDevice, d->streams[stream]));
+        arrays[a]   = a < AC_NF ? (void*)((char*)d->hi[d->in_idx[q]] + (size_t)q * d->geom.cells * es)
+                                : (void*)arr_lo(d, d->in_idx[q], q);
     }
+    /* one launch for all arrays (the buffer holds array a at a * bytes) */
+    AC_CUDA_CHECK(ac_launch_planes(arrays, plane_arrays(d), (long long)z0 * d->geom.pxy * es,
+                                   (long long)nplanes * d->geom.pxy * es, buffer, pack,
+                                   d->streams[stream], &d->launches));
     return AC_SUCCESS;
 }
 

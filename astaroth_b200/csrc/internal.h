@@ -197,6 +197,11 @@ cudaError_t ac_launch_fill(double* ptr, const long long count, const double valu
                            cudaStream_t stream, unsigned long long* launches);
 /* dst = src for `count` doubles on the device (a vectorised copy kernel when
  * both are 16-byte aligned and count is even, else cudaMemcpyAsync) */
+/* Pack (or unpack) bytes starting at offset_bytes of each of narrays (<= 16)
+ * arrays into (from) buffer + a * bytes, one launch; everything 8-byte aligned. */
+cudaError_t ac_launch_planes(void* const* arrays, const int narrays, const long long offset_bytes,
+                             const long long bytes, void* buffer, const bool pack,
+                             cudaStream_t stream, unsigned long long* launches);
 cudaError_t ac_launch_copy(const double* src, double* dst, const long long count,
                            cudaStream_t stream, unsigned long long* launches);
 /* FP32 compensated: hi/lo of `count` elements from a double value */

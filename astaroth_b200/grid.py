@@ -70,13 +70,32 @@ def slab_info(info: AcMeshInfo, z0: int, nz: int) -> AcMeshInfo:
 class LocalTransport:
     """All slabs in this process: slab i's bottom ghost planes come from slab
     i - 1's top interior planes and its top ghost planes from slab i + 1's
-    bottom interior planes (periodically)."""
+    bottom interior planes (periodically).
 
-    def exchange(self, send_bottom, send_top, recv_bottom, recv_top):
+    With `streams` (the slabs' library streams, as torch streams) the copies
+    are stream-ordered, with no host synchronisation: they run on streams[0]
+    after every slab's pack, and every slab's stream then waits for them, so
+    that the unpack follows the copies and the next pack into a send buffer
+    follows every read of it."""
+
+    def exchange(self, send_bottom, send_top, recv_bottom, recv_top, streams=None):
         k = len(send_bottom)
-        for i in range(k):
-            recv_bottom[i].copy_(send_top[(i - 1) % k])
-            recv_top[i].copy_(send_bottom[(i + 1) % k])
+        if streams is None:
+            for i in range(k):
+                recv_bottom[i].copy_(send_top[(i - 1) % k])
+                recv_top[i].copy_(send_bottom[(i + 1) % k])
+            return
+        import torch
+
+        s0 = streams[0]
+        for s in streams[1:]:
+            s0.wait_stream(s)  # every slab packed
+        with torch.cuda.stream(s0):
+            for i in range(k):
+                recv_bottom[i].copy_(send_top[(i - 1) % k])
+                recv_top[i].copy_(send_bottom[(i + 1) % k])
+        for s in streams[1:]:
+            s.wait_stream(s0)  # copies done before unpack and the next pack
 
     def combine(self, values, op):
         return {"max": max, "min": min, "sum": math.fsum}[op](values)
@@ -87,7 +106,12 @@ class DistTransport:
     bottom planes to rank - 1 (its top ghost), periodically.  Sends and
     receives are posted in the same order on every rank, so messages between
     the same two ranks match in order (world size 2 has one neighbour on both
-    sides)."""
+    sides).
+
+    With `streams` (NCCL, device buffers) the point-to-point operations are
+    enqueued behind the pack on the slab's library stream and waited for on
+    that stream (Work.wait orders the current stream, the host does not
+    block), so the unpack that follows on the same stream sees the planes."""
 
     def __init__(self):
         import torch.distributed as dist
@@ -96,8 +120,17 @@ class DistTransport:
         self.rank = dist.get_rank()
         self.world = dist.get_world_size()
 
-    def exchange(self, send_bottom, send_top, recv_bottom, recv_top):
+    def exchange(self, send_bottom, send_top, recv_bottom, recv_top, streams=None):
         (sb,), (st,), (rb,), (rt,) = send_bottom, send_top, recv_bottom, recv_top
+        if streams is None:
+            self._exchange(sb, st, rb, rt)
+            return
+        import torch
+
+        with torch.cuda.stream(streams[0]):
+            self._exchange(sb, st, rb, rt)
+
+    def _exchange(self, sb, st, rb, rt):
         if self.world == 1:
             rb.copy_(st)
             rt.copy_(sb)
@@ -145,6 +178,8 @@ class Grid:
         self.devs = [Device(slab_info(info, z0, n), device_id) for z0, n in self.ranges]
         self.plane_bytes = self.lib.acDevicePlaneBytes(self.devs[0].handle)
         dev = torch.device("cuda", device_id)
+        self._streams = [torch.cuda.ExternalStream(d.stream_handle(0), device=dev)
+                         for d in self.devs]
         self._buf = {k: [torch.empty(HALO * self.plane_bytes, dtype=torch.uint8, device=dev)
                          for _ in self.devs] for k in ("sb", "st", "rb", "rt")}
         self.cells = self.n[0] * self.n[1] * self.n[2]
@@ -179,24 +214,19 @@ class Grid:
     # ---- boundary conditions ----
     def periodic_boundconds(self) -> None:
         """Fills every ghost cell of every slab: x and y by local wrap, z by the
-        exchange with the neighbouring slabs."""
-        import torch
-
-        for d, (_, n) in zip(self.devs, self.ranges):
+        exchange with the neighbouring slabs.  Everything is ordered on the
+        slabs' library streams (stream 0); the host does not wait."""
+        b = self._buf
+        for i, (d, (_, n)) in enumerate(zip(self.devs, self.ranges)):
             nx, ny, _ = self.n
             _check(self.lib.acDevicePeriodicBoundconds(
                 d.handle, 0, Volume(0, 0, HALO), Volume(nx + 2 * HALO, ny + 2 * HALO, n + HALO)),
                 "acDevicePeriodicBoundconds")
-        b = self._buf
-        for i, (d, (_, n)) in enumerate(zip(self.devs, self.ranges)):
             _check(self.lib.acDevicePackPlanes(d.handle, 0, HALO, HALO, b["sb"][i].data_ptr()),
                    "acDevicePackPlanes")
             _check(self.lib.acDevicePackPlanes(d.handle, 0, n, HALO, b["st"][i].data_ptr()),
                    "acDevicePackPlanes")
-        for d in self.devs:
-            d.synchronize(0)
-        self.transport.exchange(b["sb"], b["st"], b["rb"], b["rt"])
-        torch.cuda.current_stream().synchronize()
+        self.transport.exchange(b["sb"], b["st"], b["rb"], b["rt"], streams=self._streams)
         for i, (d, (_, n)) in enumerate(zip(self.devs, self.ranges)):
             _check(self.lib.acDeviceUnpackPlanes(d.handle, 0, 0, HALO, b["rb"][i].data_ptr()),
                    "acDeviceUnpackPlanes")
