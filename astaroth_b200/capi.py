@@ -238,6 +238,23 @@ SIGNATURES = {
     "acDeviceFlushOutputBuffers": (C.c_int, [Device_p, C.c_int]),
     "acDeviceStoreVertexBuffer": (C.c_int, [Device_p, C.c_int, C.c_int, C.POINTER(AcMesh)]),
     "acDeviceStoreMesh": (C.c_int, [Device_p, C.c_int, C.POINTER(AcMesh)]),
+    "acDeviceLoadVertexBufferWithOffset": (C.c_int, [Device_p, C.c_int, AcMesh, C.c_int, Int3,
+                                                     Int3, C.c_int]),
+    "acDeviceLoadMeshWithOffset": (C.c_int, [Device_p, C.c_int, AcMesh, Int3, Int3, C.c_int]),
+    "acDeviceStoreVertexBufferWithOffset": (C.c_int, [Device_p, C.c_int, C.c_int, Int3, Int3,
+                                                      C.c_int, C.POINTER(AcMesh)]),
+    "acDeviceStoreMeshWithOffset": (C.c_int, [Device_p, C.c_int, Int3, Int3, C.c_int,
+                                              C.POINTER(AcMesh)]),
+    "acDeviceTransferVertexBufferWithOffset": (C.c_int, [Device_p, C.c_int, C.c_int, Int3, Int3,
+                                                         C.c_int, Device_p]),
+    "acDeviceTransferMeshWithOffset": (C.c_int, [Device_p, C.c_int, Int3, Int3, C.c_int,
+                                                 Device_p]),
+    "acDeviceTransferVertexBuffer": (C.c_int, [Device_p, C.c_int, C.c_int, Device_p]),
+    "acDeviceTransferMesh": (C.c_int, [Device_p, C.c_int, Device_p]),
+    "acDeviceUpdate": (C.c_int, [Device_p, AcMeshInfo]),
+    "acDeviceGetLocalConfig": (AcMeshInfo, [Device_p]),
+    "acDeviceVolumeCopy": (C.c_int, [Device_p, C.c_int, C.c_void_p, Volume, Volume, C.c_void_p,
+                                     Volume, Volume]),
     "acDeviceIntegrateSubstep": (C.c_int, [Device_p, C.c_int, C.c_int, Volume, Volume,
                                            C.c_double]),
     "acDevicePeriodicBoundcondStep": (C.c_int, [Device_p, C.c_int, C.c_int, Volume, Volume]),

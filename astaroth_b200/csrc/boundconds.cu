@@ -124,6 +124,65 @@ join_kernel(const Geom g, const float* __restrict__ hi, const float* __restrict_
     }
 }
 
+/* A range [first, first + count) of host-layout linear indices (pitch mx) of
+ * one field, between doubles at those indices and the (hi, lo) pair of the
+ * device layout (pitch px); the same arithmetic as split_kernel / join_kernel. */
+__device__ __forceinline__ long long
+range_dev_idx(const Geom& g, const long long L)
+{
+    const long long i = L % g.mx;
+    const long long j = (L / g.mx) % g.my;
+    const long long k = L / ((long long)g.mx * g.my);
+    return i + j * g.px + k * g.pxy;
+}
+
+__global__ void
+split_range_kernel(const Geom g, const double* __restrict__ src, float* __restrict__ hi,
+                   float* __restrict__ lo, const long long first, const long long count)
+{
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < count;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long L = first + t;
+        const long long d = range_dev_idx(g, L);
+        const double v    = src[L];
+        const float vh    = (float)v;
+        hi[d]             = vh;
+        lo[d]             = (float)(v - (double)vh);
+    }
+}
+
+__global__ void
+join_range_kernel(const Geom g, const float* __restrict__ hi, const float* __restrict__ lo,
+                  double* __restrict__ dst, const long long first, const long long count)
+{
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < count;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long L = first + t;
+        const long long d = range_dev_idx(g, L);
+        dst[L]            = (double)hi[d] + (double)lo[d];
+    }
+}
+
+/* out[(p + out_offset) in out_volume] = in[(p + in_offset) in in_volume] for p
+ * in the box nn, x fastest (the reference's AC_VOLUME_COPY,
+ * acc-runtime/built-in/kernels.h:43-67). */
+__global__ void
+volume_copy_kernel(const double* __restrict__ in, const Volume in_offset, const Volume in_volume,
+                   double* __restrict__ out, const Volume out_offset, const Volume out_volume,
+                   const Volume nn)
+{
+    const long long total = (long long)nn.x * nn.y * nn.z;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const long long x = t % nn.x, y = (t / nn.x) % nn.y, z = t / ((long long)nn.x * nn.y);
+        const long long si = (x + in_offset.x) + (long long)(y + in_offset.y) * in_volume.x +
+                             (long long)(z + in_offset.z) * in_volume.x * in_volume.y;
+        const long long di = (x + out_offset.x) + (long long)(y + out_offset.y) * out_volume.x +
+                             (long long)(z + out_offset.z) * out_volume.x * out_volume.y;
+        out[di] = in[si];
+    }
+}
+
 /* Plane ranges of up to 16 arrays to or from one contiguous buffer, in 8-byte
  * words: word w of array a is arrays[a][offset + w] and buffer[a * count + w]
  * (pack) or the reverse (unpack); grid-stride over all arrays' words. */
@@ -271,6 +330,47 @@ ac_launch_planes(void* const* arrays, const int narrays, const long long offset_
     const long long count = bytes / 8;
     planes_kernel<<<grid_for((long long)narrays * count, 256), 256, 0, stream>>>(
         arr, narrays, offset_bytes / 8, count, (unsigned long long*)buffer, pack);
+    if (launches)
+        ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t
+ac_launch_split_range(const Geom& g, const double* src, float* hi, float* lo,
+                      const long long first, const long long count, cudaStream_t stream,
+                      unsigned long long* launches)
+{
+    if (count <= 0)
+        return cudaSuccess;
+    split_range_kernel<<<grid_for(count, 256), 256, 0, stream>>>(g, src, hi, lo, first, count);
+    if (launches)
+        ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t
+ac_launch_join_range(const Geom& g, const float* hi, const float* lo, double* dst,
+                     const long long first, const long long count, cudaStream_t stream,
+                     unsigned long long* launches)
+{
+    if (count <= 0)
+        return cudaSuccess;
+    join_range_kernel<<<grid_for(count, 256), 256, 0, stream>>>(g, hi, lo, dst, first, count);
+    if (launches)
+        ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t
+ac_launch_volume_copy(const double* in, const Volume in_offset, const Volume in_volume,
+                      double* out, const Volume out_offset, const Volume out_volume,
+                      const Volume nn, cudaStream_t stream, unsigned long long* launches)
+{
+    const long long total = (long long)nn.x * nn.y * nn.z;
+    if (total <= 0)
+        return cudaSuccess;
+    volume_copy_kernel<<<grid_for(total, 256), 256, 0, stream>>>(in, in_offset, in_volume, out,
+                                                                out_offset, out_volume, nn);
     if (launches)
         ++*launches;
     return cudaGetLastError();

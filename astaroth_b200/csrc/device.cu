@@ -629,6 +629,254 @@ acDeviceStoreMesh(const Device d, const Stream stream, AcMesh* host_mesh)
     return res;
 }
 
+/* ---- linear ranges between meshes: the reference's *WithOffset family
+ * (src/core/device.cc:666-698 and its store and transfer counterparts).
+ * num_vertices consecutive values in host-layout linear order (x fastest,
+ * rows of mx) move from position src of the source to position dst of the
+ * target, into or out of the device's in-buffer.  FP32-compensated devices
+ * split/join the range on the fly.  Ranges must lie inside both meshes. ---- */
+
+static bool
+mesh_dims(const AcMeshInfo& info, long long m[3])
+{
+    AcMeshInfo h = info;
+    if (acHostUpdateParams(&h) != AC_SUCCESS)
+        return false;
+    const int3 v = h.int3_params[AC_mlocal];
+    m[0]         = v.x;
+    m[1]         = v.y;
+    m[2]         = v.z;
+    return v.x > 0 && v.y > 0 && v.z > 0;
+}
+
+/* linear index of p in a mesh of dims m, or -1 when p is outside or the n
+ * values from it do not fit */
+static long long
+range_start(const int3 p, const long long m[3], const long long n)
+{
+    if (n < 0 || p.x < 0 || p.y < 0 || p.z < 0 || p.x >= m[0] || p.y >= m[1] || p.z >= m[2])
+        return -1;
+    const long long L = p.x + m[0] * (p.y + m[1] * (long long)p.z);
+    return L + n <= m[0] * m[1] * m[2] ? L : -1;
+}
+
+static void
+device_dims(const Device d, long long m[3])
+{
+    m[0] = d->geom.mx;
+    m[1] = d->geom.my;
+    m[2] = d->geom.mz;
+}
+
+extern "C" AcResult
+acDeviceLoadVertexBufferWithOffset(const Device d, const Stream stream, const AcMesh host_mesh,
+                                   const VertexBufferHandle h, const int3 src, const int3 dst,
+                                   const int num_vertices)
+{
+    if (!d || !stream_ok(stream) || (int)h < 0 || h >= NUM_VTXBUF_HANDLES)
+        return AC_FAILURE;
+    if (!host_mesh.vertex_buffer[h])
+        return AC_NOT_ALLOCATED;
+    long long hm[3], dm[3];
+    device_dims(d, dm);
+    if (!mesh_dims(host_mesh.info, hm))
+        return AC_FAILURE;
+    const long long n = num_vertices, s0 = range_start(src, hm, n), d0 = range_start(dst, dm, n);
+    if (s0 < 0 || d0 < 0)
+        return AC_FAILURE;
+    if (n == 0)
+        return AC_SUCCESS;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    const int b       = d->in_idx[h];
+    cudaStream_t st   = d->streams[stream];
+    const double* hp  = host_mesh.vertex_buffer[h] + s0;
+    if (d->precision == 0) {
+        AC_CUDA_CHECK(cudaMemcpyAsync(arr64(d, b, h) + d0, hp, n * sizeof(double),
+                                      cudaMemcpyHostToDevice, st));
+        return AC_SUCCESS;
+    }
+    AC_CUDA_CHECK(cudaMemcpyAsync(d->staging + d0, hp, n * sizeof(double), cudaMemcpyHostToDevice,
+                                  st));
+    AC_CUDA_CHECK(ac_launch_split_range(d->geom, d->staging, arr_hi(d, b, h), arr_lo(d, b, h),
+                                        d0, n, st, &d->launches));
+    AC_CUDA_CHECK(cudaStreamSynchronize(st)); /* the staging field is shared */
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceLoadMeshWithOffset(const Device d, const Stream stream, const AcMesh host_mesh,
+                           const int3 src, const int3 dst, const int num_vertices)
+{
+    AcResult res = AC_SUCCESS;
+    for (int q = 0; q < AC_NF; ++q)
+        res = worst(res, acDeviceLoadVertexBufferWithOffset(d, stream, host_mesh,
+                                                            (VertexBufferHandle)q, src, dst,
+                                                            num_vertices));
+    return res;
+}
+
+extern "C" AcResult
+acDeviceStoreVertexBufferWithOffset(const Device d, const Stream stream,
+                                    const VertexBufferHandle h, const int3 src, const int3 dst,
+                                    const int num_vertices, AcMesh* host_mesh)
+{
+    if (!d || !host_mesh || !stream_ok(stream) || (int)h < 0 || h >= NUM_VTXBUF_HANDLES)
+        return AC_FAILURE;
+    if (!host_mesh->vertex_buffer[h])
+        return AC_NOT_ALLOCATED;
+    long long hm[3], dm[3];
+    device_dims(d, dm);
+    if (!mesh_dims(host_mesh->info, hm))
+        return AC_FAILURE;
+    const long long n = num_vertices, s0 = range_start(src, dm, n), d0 = range_start(dst, hm, n);
+    if (s0 < 0 || d0 < 0)
+        return AC_FAILURE;
+    if (n == 0)
+        return AC_SUCCESS;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    const int b     = d->in_idx[h];
+    cudaStream_t st = d->streams[stream];
+    double* hp      = host_mesh->vertex_buffer[h] + d0;
+    if (d->precision == 0) {
+        AC_CUDA_CHECK(cudaMemcpyAsync(hp, arr64(d, b, h) + s0, n * sizeof(double),
+                                      cudaMemcpyDeviceToHost, st));
+    }
+    else {
+        AC_CUDA_CHECK(ac_launch_join_range(d->geom, arr_hi(d, b, h), arr_lo(d, b, h), d->staging,
+                                           s0, n, st, &d->launches));
+        AC_CUDA_CHECK(cudaMemcpyAsync(hp, d->staging + s0, n * sizeof(double),
+                                      cudaMemcpyDeviceToHost, st));
+    }
+    AC_CUDA_CHECK(cudaStreamSynchronize(st)); /* the host range is ready on return */
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceStoreMeshWithOffset(const Device d, const Stream stream, const int3 src, const int3 dst,
+                            const int num_vertices, AcMesh* host_mesh)
+{
+    AcResult res = AC_SUCCESS;
+    for (int q = 0; q < AC_NF; ++q)
+        res = worst(res, acDeviceStoreVertexBufferWithOffset(d, stream, (VertexBufferHandle)q, src,
+                                                             dst, num_vertices, host_mesh));
+    return res;
+}
+
+/* Device to device (the reference's acDeviceTransfer*, device.cc): on the source
+ * device's stream, with a peer copy between GPUs.  Both devices must have the
+ * same precision. */
+extern "C" AcResult
+acDeviceTransferVertexBufferWithOffset(const Device from, const Stream stream,
+                                       const VertexBufferHandle h, const int3 src, const int3 dst,
+                                       const int num_vertices, Device to)
+{
+    if (!from || !to || !stream_ok(stream) || (int)h < 0 || h >= NUM_VTXBUF_HANDLES ||
+        from->precision != to->precision)
+        return AC_FAILURE;
+    long long fm[3], tm[3];
+    device_dims(from, fm);
+    device_dims(to, tm);
+    const long long n = num_vertices, s0 = range_start(src, fm, n), d0 = range_start(dst, tm, n);
+    if (s0 < 0 || d0 < 0)
+        return AC_FAILURE;
+    if (n == 0)
+        return AC_SUCCESS;
+    AC_CUDA_CHECK(cudaSetDevice(from->id));
+    cudaStream_t st = from->streams[stream];
+    const int fb = from->in_idx[h], tb = to->in_idx[h];
+    if (from->precision == 0) {
+        AC_CUDA_CHECK(cudaMemcpyPeerAsync(arr64(to, tb, h) + d0, to->id, arr64(from, fb, h) + s0,
+                                          from->id, n * sizeof(double), st));
+        return AC_SUCCESS;
+    }
+    /* FP32-compensated: join into the source's staging field, copy the doubles
+     * to the target's staging field, split there */
+    AC_CUDA_CHECK(ac_launch_join_range(from->geom, arr_hi(from, fb, h), arr_lo(from, fb, h),
+                                       from->staging, s0, n, st, &from->launches));
+    AC_CUDA_CHECK(cudaMemcpyPeerAsync(to->staging + d0, to->id, from->staging + s0, from->id,
+                                      n * sizeof(double), st));
+    AC_CUDA_CHECK(cudaStreamSynchronize(st));
+    AC_CUDA_CHECK(cudaSetDevice(to->id));
+    cudaStream_t tst = to->streams[stream];
+    AC_CUDA_CHECK(ac_launch_split_range(to->geom, to->staging, arr_hi(to, tb, h),
+                                        arr_lo(to, tb, h), d0, n, tst, &to->launches));
+    AC_CUDA_CHECK(cudaStreamSynchronize(tst));
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceTransferMeshWithOffset(const Device from, const Stream stream, const int3 src,
+                               const int3 dst, const int num_vertices, Device to)
+{
+    AcResult res = AC_SUCCESS;
+    for (int q = 0; q < AC_NF; ++q)
+        res = worst(res, acDeviceTransferVertexBufferWithOffset(from, stream, (VertexBufferHandle)q,
+                                                                src, dst, num_vertices, to));
+    return res;
+}
+
+extern "C" AcResult
+acDeviceTransferVertexBuffer(const Device from, const Stream stream, const VertexBufferHandle h,
+                             Device to)
+{
+    if (!from || !to || from->geom.mx != to->geom.mx || from->geom.my != to->geom.my ||
+        from->geom.mz != to->geom.mz)
+        return AC_FAILURE;
+    const long long n = (long long)from->geom.mx * from->geom.my * from->geom.mz;
+    if (n > 0x7fffffffLL)
+        return AC_FAILURE;
+    const int3 o = {0, 0, 0};
+    return acDeviceTransferVertexBufferWithOffset(from, stream, h, o, o, (int)n, to);
+}
+
+extern "C" AcResult
+acDeviceTransferMesh(const Device from, const Stream stream, Device to)
+{
+    AcResult res = AC_SUCCESS;
+    for (int q = 0; q < AC_NF; ++q)
+        res = worst(res, acDeviceTransferVertexBuffer(from, stream, (VertexBufferHandle)q, to));
+    return res;
+}
+
+/* acDeviceUpdate / acDeviceGetLocalConfig (include/astaroth_device.h:217,246):
+ * the same as acDeviceLoadMeshInfo / acDeviceGetConfig on one GPU. */
+extern "C" AcResult
+acDeviceUpdate(Device d, const AcMeshInfo info)
+{
+    return acDeviceLoadMeshInfo(d, info);
+}
+
+extern "C" AcMeshInfo
+acDeviceGetLocalConfig(const Device d)
+{
+    return acDeviceGetConfig(d);
+}
+
+/* acDeviceVolumeCopy (include/astaroth_device.h:235, acc-runtime/api/
+ * common_kernels.cc:143-155): copies the box min(in_volume, out_volume) from
+ * in at in_offset to out at out_offset, both arrays laid out x fastest with
+ * their volume's dims.  Unlike the reference, a box that would reach past
+ * either array is refused. */
+extern "C" AcResult
+acDeviceVolumeCopy(const Device d, const Stream stream, const AcReal* in, const Volume in_offset,
+                   const Volume in_volume, AcReal* out, const Volume out_offset,
+                   const Volume out_volume)
+{
+    if (!d || !in || !out || !stream_ok(stream))
+        return AC_FAILURE;
+    const Volume nn = {in_volume.x < out_volume.x ? in_volume.x : out_volume.x,
+                       in_volume.y < out_volume.y ? in_volume.y : out_volume.y,
+                       in_volume.z < out_volume.z ? in_volume.z : out_volume.z};
+    if (in_offset.x + nn.x > in_volume.x || in_offset.y + nn.y > in_volume.y ||
+        in_offset.z + nn.z > in_volume.z || out_offset.x + nn.x > out_volume.x ||
+        out_offset.y + nn.y > out_volume.y || out_offset.z + nn.z > out_volume.z)
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    AC_CUDA_CHECK(ac_launch_volume_copy(in, in_offset, in_volume, out, out_offset, out_volume, nn,
+                                        d->streams[stream], &d->launches));
+    return AC_SUCCESS;
+}
+
 extern "C" AcResult
 acDeviceSetVertexBuffer(const Device d, const Stream stream, const VertexBufferHandle h,
                         const AcReal value)

@@ -202,6 +202,19 @@ cudaError_t ac_launch_fill(double* ptr, const long long count, const double valu
 cudaError_t ac_launch_planes(void* const* arrays, const int narrays, const long long offset_bytes,
                              const long long bytes, void* buffer, const bool pack,
                              cudaStream_t stream, unsigned long long* launches);
+/* Host-layout linear range [first, first + count) of one field: doubles at
+ * those indices of src/dst <-> (hi, lo) in the FP32 device layout. */
+cudaError_t ac_launch_split_range(const Geom& g, const double* src, float* hi, float* lo,
+                                  const long long first, const long long count,
+                                  cudaStream_t stream, unsigned long long* launches);
+cudaError_t ac_launch_join_range(const Geom& g, const float* hi, const float* lo, double* dst,
+                                 const long long first, const long long count,
+                                 cudaStream_t stream, unsigned long long* launches);
+/* The box nn from in (offset in_offset in an in_volume array) to out. */
+cudaError_t ac_launch_volume_copy(const double* in, const Volume in_offset,
+                                  const Volume in_volume, double* out, const Volume out_offset,
+                                  const Volume out_volume, const Volume nn, cudaStream_t stream,
+                                  unsigned long long* launches);
 cudaError_t ac_launch_copy(const double* src, double* dst, const long long count,
                            cudaStream_t stream, unsigned long long* launches);
 /* FP32 compensated: hi/lo of `count` elements from a double value */
