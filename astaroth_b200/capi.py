@@ -251,6 +251,10 @@ SIGNATURES = {
                                                  Device_p]),
     "acDeviceTransferVertexBuffer": (C.c_int, [Device_p, C.c_int, C.c_int, Device_p]),
     "acDeviceTransferMesh": (C.c_int, [Device_p, C.c_int, Device_p]),
+    "acDeviceStoreVectorUniform": (C.c_int, [Device_p, C.c_int, C.c_int, C.POINTER(Real3)]),
+    "acDeviceStoreIntUniform": (C.c_int, [Device_p, C.c_int, C.c_int, C.POINTER(C.c_int)]),
+    "acDeviceStoreInt3Uniform": (C.c_int, [Device_p, C.c_int, C.c_int, C.POINTER(Int3)]),
+    "acDeviceLoadInt3Uniform": (C.c_int, [Device_p, C.c_int, C.c_int, Int3]),
     "acDeviceUpdate": (C.c_int, [Device_p, AcMeshInfo]),
     "acDeviceGetLocalConfig": (AcMeshInfo, [Device_p]),
     "acDeviceVolumeCopy": (C.c_int, [Device_p, C.c_int, C.c_void_p, Volume, Volume, C.c_void_p,

@@ -481,6 +481,22 @@ acDeviceLoadVectorUniform(const Device d, const Stream stream, const AcReal3Para
     return refresh_config(d, info);
 }
 
+/* include/astaroth_device.h device_load_uniform_decl.h: an int3 parameter.
+ * The mesh dimensions and offsets cannot change after acDeviceCreate, so
+ * this serves the parameters derived from them being loaded unchanged, as
+ * the reference's grid layer does. */
+extern "C" AcResult
+acDeviceLoadInt3Uniform(const Device d, const Stream stream, const AcInt3Param param,
+                        const int3 value)
+{
+    (void)stream;
+    if (!d || (int)param < 0 || param >= NUM_INT3_PARAMS)
+        return AC_FAILURE;
+    AcMeshInfo info          = d->config;
+    info.int3_params[param] = value;
+    return refresh_config(d, info);
+}
+
 extern "C" AcResult
 acDeviceLoadIntUniform(const Device d, const Stream stream, const AcIntParam param,
                        const int value)
@@ -494,6 +510,39 @@ acDeviceLoadIntUniform(const Device d, const Stream stream, const AcIntParam par
     if (r == AC_SUCCESS)
         d->solve_variant = d->config.int_params[AC_debug_plain_kernel] ? 0 : 1;
     return r;
+}
+
+/* include/astaroth_device.h:61 and device_store_uniform_decl.h. */
+extern "C" AcResult
+acDeviceStoreVectorUniform(const Device d, const Stream stream, const AcReal3Param param,
+                           AcReal3* value)
+{
+    (void)stream;
+    if (!d || !value || (int)param < 0 || param >= NUM_REAL3_PARAMS)
+        return AC_FAILURE;
+    *value = d->config.real3_params[param];
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceStoreIntUniform(const Device d, const Stream stream, const AcIntParam param, int* value)
+{
+    (void)stream;
+    if (!d || !value || (int)param < 0 || param >= NUM_INT_PARAMS)
+        return AC_FAILURE;
+    *value = d->config.int_params[param];
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceStoreInt3Uniform(const Device d, const Stream stream, const AcInt3Param param,
+                         int3* value)
+{
+    (void)stream;
+    if (!d || !value || (int)param < 0 || param >= NUM_INT3_PARAMS)
+        return AC_FAILURE;
+    *value = d->config.int3_params[param];
+    return AC_SUCCESS;
 }
 
 extern "C" AcResult

@@ -116,6 +116,20 @@ def test_update_and_local_config():
         assert lib.acDeviceUpdate(d.handle, cfg) == 0
         assert lib.acDeviceGetConfig(d.handle).real_params[capi.RealParam.AC_nu_visc] == 3e-3
         assert lib.acDeviceGetLocalConfig(d.handle).real_params[capi.RealParam.AC_nu_visc] == 3e-3
+        ds, iv, n3 = capi.Real3(), C.c_int(), Int3()
+        assert lib.acDeviceStoreVectorUniform(d.handle, 0, capi.Real3Param.AC_ds, C.byref(ds)) == 0
+        assert ds.x == info.real3_params[capi.Real3Param.AC_ds].x
+        assert lib.acDeviceStoreIntUniform(d.handle, 0, capi.IntParam.AC_precision,
+                                           C.byref(iv)) == 0 and iv.value == 0
+        assert lib.acDeviceStoreInt3Uniform(d.handle, 0, capi.Int3Param.AC_nlocal,
+                                            C.byref(n3)) == 0
+        assert (n3.x, n3.y, n3.z) == SHAPE
+        # the offset may be reloaded; the dimensions may not change
+        assert lib.acDeviceLoadInt3Uniform(d.handle, 0, capi.Int3Param.AC_multigpu_offset,
+                                           Int3(0, 0, 0)) == 0
+        assert lib.acDeviceLoadInt3Uniform(d.handle, 0, capi.Int3Param.AC_nlocal,
+                                           Int3(20, 14, 13)) == capi.AC_FAILURE
+        assert lib.acDeviceStoreIntUniform(d.handle, 0, 99, C.byref(iv)) == capi.AC_FAILURE
 
 
 def test_volume_copy():
