@@ -7,7 +7,7 @@
  * a chunk of up to ZCHUNK planes (fewer on small meshes, so that the grid
  * still covers the SMs; see zchunk_for).  A ring of RING = 8 shared-memory slots holds the
  * planes z-3 .. z+3 the stencils of plane z need plus one plane in flight.
- * One TMA instruction (cp.async.bulk.tensor.4d, no multicast) brings a whole
+ * One TMA instruction (cp.async.bulk.tensor.4d, CTA-local) brings a whole
  * plane of all 8 fields -- a (38 x 10 x 1 x 8) box of the in-buffer (40 wide
  * in FP32, where the box row must be a multiple of 16 bytes), halo
  * included -- into a slot and signals an mbarrier; every cell value is read

@@ -1,7 +1,7 @@
 /*
  * Shared-memory plane ring plumbing of the tiled substep kernels: mbarrier
  * waits with an iteration bound, and the 4-D TMA plane load
- * (cp.async.bulk.tensor, no multicast) completing on an mbarrier.
+ * (cp.async.bulk.tensor into this CTA only) completing on an mbarrier.
  */
 #pragma once
 
