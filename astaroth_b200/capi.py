@@ -255,6 +255,8 @@ SIGNATURES = {
     "acDeviceStoreIntUniform": (C.c_int, [Device_p, C.c_int, C.c_int, C.POINTER(C.c_int)]),
     "acDeviceStoreInt3Uniform": (C.c_int, [Device_p, C.c_int, C.c_int, C.POINTER(Int3)]),
     "acDeviceLoadInt3Uniform": (C.c_int, [Device_p, C.c_int, C.c_int, Int3]),
+    "acDeviceLoadMeshStaged": (C.c_int, [Device_p, C.c_int, AcMesh]),
+    "acDeviceCommitStagedMesh": (C.c_int, [Device_p, C.c_int]),
     "acDeviceUpdate": (C.c_int, [Device_p, AcMeshInfo]),
     "acDeviceGetLocalConfig": (AcMeshInfo, [Device_p]),
     "acDeviceVolumeCopy": (C.c_int, [Device_p, C.c_int, C.c_void_p, Volume, Volume, C.c_void_p,

@@ -248,6 +248,11 @@ release(Device d)
     cudaFree(d->adj_pgrad);
     cudaFree(d->adj_tape);
     cudaFree(d->bfield);
+    cudaFree(d->stage);
+    if (d->stage_loaded)
+        cudaEventDestroy(d->stage_loaded);
+    if (d->stage_read)
+        cudaEventDestroy(d->stage_read);
     cudaFreeHost(d->host_result);
     for (int s = 0; s < NUM_STREAMS; ++s)
         if (d->streams[s])
@@ -923,6 +928,78 @@ acDeviceVolumeCopy(const Device d, const Stream stream, const AcReal* in, const 
     AC_CUDA_CHECK(cudaSetDevice(d->id));
     AC_CUDA_CHECK(ac_launch_volume_copy(in, in_offset, in_volume, out, out_offset, out_volume, nn,
                                         d->streams[stream], &d->launches));
+    return AC_SUCCESS;
+}
+
+/* ---- pipelined loads of whole meshes ----
+ * acDeviceLoadMeshStaged copies a host mesh into a device-side stage on
+ * `stream` and returns at once; acDeviceCommitStagedMesh makes `stream` wait
+ * for that copy and moves the stage into the in-buffer (a device copy, or the
+ * hi/lo split of FP32-compensated meshes).  A caller that integrates on one
+ * stream and stages the next input on another overlaps the host transfer
+ * with the integration; the next staged load waits until the commit has read
+ * the stage.  Host buffers must be page-locked for the copy to run
+ * asynchronously. */
+static cudaError_t
+ensure_stage(Device d)
+{
+    if (d->stage)
+        return cudaSuccess;
+    const size_t n = (size_t)d->geom.mx * d->geom.my * d->geom.mz;
+    cudaError_t e  = cudaMalloc((void**)&d->stage, AC_NF * n * sizeof(double));
+    if (e != cudaSuccess)
+        return e;
+    e = cudaEventCreateWithFlags(&d->stage_loaded, cudaEventDisableTiming);
+    if (e != cudaSuccess)
+        return e;
+    return cudaEventCreateWithFlags(&d->stage_read, cudaEventDisableTiming);
+}
+
+extern "C" AcResult
+acDeviceLoadMeshStaged(const Device d, const Stream stream, const AcMesh host_mesh)
+{
+    if (!d || !stream_ok(stream))
+        return AC_FAILURE;
+    for (int q = 0; q < AC_NF; ++q)
+        if (!host_mesh.vertex_buffer[q])
+            return AC_NOT_ALLOCATED;
+    if (!host_matches(d, host_mesh.info)) {
+        fprintf(stderr, "astaroth_b200: host mesh dimensions differ from the device's\n");
+        return AC_FAILURE;
+    }
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    const bool first = d->stage == nullptr;
+    AC_CUDA_CHECK(ensure_stage(d));
+    cudaStream_t st = d->streams[stream];
+    if (!first) /* the previous commit has read the stage */
+        AC_CUDA_CHECK(cudaStreamWaitEvent(st, d->stage_read, 0));
+    const size_t n = (size_t)d->geom.mx * d->geom.my * d->geom.mz;
+    for (int q = 0; q < AC_NF; ++q)
+        AC_CUDA_CHECK(cudaMemcpyAsync(d->stage + q * n, host_mesh.vertex_buffer[q],
+                                      n * sizeof(double), cudaMemcpyHostToDevice, st));
+    AC_CUDA_CHECK(cudaEventRecord(d->stage_loaded, st));
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDeviceCommitStagedMesh(const Device d, const Stream stream)
+{
+    if (!d || !stream_ok(stream) || !d->stage)
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    cudaStream_t st = d->streams[stream];
+    AC_CUDA_CHECK(cudaStreamWaitEvent(st, d->stage_loaded, 0));
+    const size_t n = (size_t)d->geom.mx * d->geom.my * d->geom.mz;
+    for (int q = 0; q < AC_NF; ++q) {
+        const int b = d->in_idx[q];
+        if (d->precision == 0)
+            AC_CUDA_CHECK(ac_launch_copy(d->stage + q * n, arr64(d, b, q), (long long)n, st,
+                                         &d->launches));
+        else
+            AC_CUDA_CHECK(ac_launch_split(d->geom, d->stage + q * n, arr_hi(d, b, q),
+                                          arr_lo(d, b, q), st, &d->launches));
+    }
+    AC_CUDA_CHECK(cudaEventRecord(d->stage_read, st));
     return AC_SUCCESS;
 }
 

@@ -182,6 +182,12 @@ struct device_s {
      * the next launch that recomputes the CFL words */
     double outputs[NUM_REAL_OUTPUTS];
     unsigned out_set;
+    /* acDeviceLoadMeshStaged: a device copy of a whole host mesh (8 fields of
+     * mx*my*mz doubles, host layout), allocated on first use; stage_loaded is
+     * recorded after its copy from the host, stage_read after the commit has
+     * read it */
+    double* stage;
+    cudaEvent_t stage_loaded, stage_read;
     unsigned long long launches;
 };
 
