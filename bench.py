@@ -167,6 +167,17 @@ def profile_traffic(name: str):
     return None
 
 
+def profile_limiter(name: str):
+    """The `limiter:` line of profiles/<name>: what ncu showed bounding the kernel."""
+    p = ROOT / "profiles" / name
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.strip().startswith("limiter:"):
+            return line.split(":", 1)[1].strip()
+    return None
+
+
 def cpu_reference_sample(n: int, steps: int = 1):
     """Times the reference's host model (oracle/_ref, else the port) on an n^3 sample."""
     from oracle import oracle  # checker only: the CPU baseline leg
@@ -379,7 +390,8 @@ def run_gpu(args):
                                            "256^3 scaled by the cell count to 512^3)",
                          "bytes_per_cell_step": BYTES_PER_CELL_STEP["fp64"],
                          "peak_source": peak_kind, "solve_ms_per_step": solve_step_ms,
-                         "boundconds_ms_per_step": sum(bc_ms[-3:])},
+                         "boundconds_ms_per_step": sum(bc_ms[-3:]),
+                         "limiter": profile_limiter("solve_tiled_fp64_256.md")},
             "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
             "fp32comp": fp32, "ensemble": ens,
         }
