@@ -84,7 +84,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     sample_src = CSRC / "ac_devicetest.c"
     if sample_src.exists() and (force or _stale(SAMPLE, [sample_src, LIB])):
         _run(["gcc", "-O2", "-std=c11", f"-I{INCLUDE}", str(sample_src), "-o", str(SAMPLE),
-              f"-L{PKG}", "-lastaroth_b200", f"-Wl,-rpath,{PKG}", "-lm"], verbose)
+              f"-L{PKG}", "-lastaroth_b200", "-Wl,-rpath,$ORIGIN", "-lm"], verbose)
     return LIB
 
 
