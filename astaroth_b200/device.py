@@ -169,6 +169,25 @@ class Device:
         _check(self.lib.acDeviceStoreMesh(self._h, stream, C.byref(m)), "acDeviceStoreMesh")
         return out
 
+    def load_mesh_staged(self, fields: np.ndarray, stream: int = 1) -> None:
+        """acDeviceLoadMeshStaged: starts the copy of `fields` into the device-side
+        stage and returns.  `fields` must stay alive (and should be page-locked,
+        e.g. a pinned torch tensor's numpy view) until commit_staged."""
+        self._staged = fields  # keeps the host array alive while the copy runs
+        _check(self.lib.acDeviceLoadMeshStaged(self._h, stream, mesh_struct(fields, self.info)),
+               "acDeviceLoadMeshStaged")
+
+    def commit_staged(self, stream: int = 0) -> None:
+        """acDeviceCommitStagedMesh: `stream` waits for the staged copy, then the
+        stage becomes the in-buffer."""
+        _check(self.lib.acDeviceCommitStagedMesh(self._h, stream), "acDeviceCommitStagedMesh")
+
+    def transfer_mesh(self, other: "Device", stream: int = 0) -> None:
+        """acDeviceTransferMesh: this device's in-buffer into other's (equal dims
+        and precision), on this device's stream."""
+        _check(self.lib.acDeviceTransferMesh(self._h, stream, other.handle),
+               "acDeviceTransferMesh")
+
     def swap_buffers(self) -> None:
         _check(self.lib.acDeviceSwapBuffers(self._h), "acDeviceSwapBuffers")
 

@@ -198,3 +198,13 @@ def test_staged_loads_overlap_and_equal_direct_loads(precision):
         assert lib.acDeviceLoadMeshStaged(d.handle, 1, bad) == capi.AC_NOT_ALLOCATED
     for a, b in zip(direct, staged):
         assert np.array_equal(a, b)
+
+    # the same through the Python wrappers
+    with ab.Device(info) as d, ab.Device(info) as e:
+        d.load_mesh_staged(pinned[1].numpy())
+        d.commit_staged()
+        d.integrate_step(1e-3)
+        d.synchronize()
+        d.transfer_mesh(e)
+        d.synchronize()
+        assert np.array_equal(e.store_mesh(), direct[1])
