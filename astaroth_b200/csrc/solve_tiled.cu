@@ -435,10 +435,11 @@ bool
 ac_tiled_supported(const Geom& g, const int precision)
 {
     /* TMA: global strides must be multiples of 16 bytes and the box must not
-     * exceed the tensor (mx >= box width, my >= 10). */
+     * exceed the tensor, whose rows are the px-element pitch (px >= box width,
+     * my >= 10; an FP32 row of mx = 38 has px = 40, so 32^3 meshes qualify). */
     const int esz = precision == 0 ? 8 : 4;
     const int hxp = precision == 0 ? Tile<double>::HXP : Tile<float>::HXP;
-    return ((long long)g.px * esz) % 16 == 0 && g.mx >= hxp && g.my >= HY && g.nx >= TX &&
+    return ((long long)g.px * esz) % 16 == 0 && g.px >= hxp && g.my >= HY && g.nx >= TX &&
            g.ny >= TY;
 }
 
@@ -450,7 +451,9 @@ ac_encode_field_map(void* map_out, void* base, const Geom& g, const int precisio
     if (!fn)
         return false;
     const size_t esz            = precision == 0 ? sizeof(double) : sizeof(float);
-    const cuuint64_t dims[4]    = {(cuuint64_t)g.mx, (cuuint64_t)g.my, (cuuint64_t)g.mz,
+    /* rows of px elements: the padding of FP32 rows (px - mx <= 3 elements,
+     * allocated and never written) may be read into unused box columns */
+    const cuuint64_t dims[4]    = {(cuuint64_t)g.px, (cuuint64_t)g.my, (cuuint64_t)g.mz,
                                    (cuuint64_t)AC_NF};
     const cuuint64_t strides[3] = {(cuuint64_t)g.px * esz, (cuuint64_t)g.pxy * esz,
                                    (cuuint64_t)g.cells * esz};

@@ -90,9 +90,12 @@ def test_compensated_error_well_inside_bar():
     assert err.max() <= 1e-6, err
 
 
-def test_plain_and_tiled_fp32comp_agree():
-    a = run((64, 40, 24), 6, 2, precision=1, plain=True)
-    b = run((64, 40, 24), 6, 2, precision=1, plain=False)
+@pytest.mark.parametrize("n", [(64, 40, 24), 32, (33, 20, 12)])
+def test_plain_and_tiled_fp32comp_agree(n):
+    """Including rows of mx = 38 and 39, whose 40-element pitch holds the tiled
+    kernel's 40-wide plane box."""
+    a = run(n, 6, 2, precision=1, plain=True)
+    b = run(n, 6, 2, precision=1, plain=False)
     err = oracle.rel_linf(a, b)
     assert err.max() <= 1e-8, err
 
