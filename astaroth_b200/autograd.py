@@ -8,7 +8,10 @@ checkpoint, keeping the three substep states f_0, f_1, f_2 of every step
 (acDeviceAdjointTapeForward); then for each step (last first) the discrete
 adjoint substeps s = 2, 1, 0 are applied (acDeviceAdjointTapeBackward, i.e.
 acDeviceIntegrateSubstepAdjoint about the taped states).  Every step is
-recomputed once.  Memory: N/k checkpoints plus 3k substep states.
+recomputed once, except the last segment: the forward pass integrates it
+through the tape already, and the backward pass uses those states unless the
+device's tape was written since.  Memory: N/k checkpoints plus 3k substep
+states.
 
 Tensors are (8, mz, my, mx) float64 on the GPU (halos included, as the host
 AcMesh).  The integration fills the halos itself, so gradients live on the
@@ -21,7 +24,7 @@ import math
 import torch
 
 from . import capi
-from .device import Device
+from .device import AstarothError, Device
 
 D1 = (3 / 4, -3 / 20, 1 / 60)
 
@@ -64,14 +67,24 @@ class _Integrate(torch.autograd.Function):
         dev.set_real(capi.RealParam.AC_eta, float(eta))
         dev.load_mesh_device(f0.contiguous())
         ckpts = [f0.detach().clone()]
+        last0 = (steps - 1) // every * every  # first step of the last segment
+        token = None
         for n in range(steps):
+            if tape and n == last0:
+                # the last segment through the tape, whose substep states the
+                # backward pass then uses without integrating it again
+                try:
+                    token = dev.adjoint_tape_forward(steps - last0, dt)
+                    break
+                except AstarothError:
+                    pass  # no adjoint on this device (FP32, upwinding): plain steps
             dev.integrate_step(dt)
             if (n + 1) % every == 0 and n + 1 < steps:
                 ckpts.append(dev.store_mesh_device(torch.empty_like(f0)))
         out = dev.store_mesh_device(torch.empty_like(f0))
         torch.cuda.synchronize()
         ctx.dev, ctx.steps, ctx.dt, ctx.every, ctx.ckpts = dev, steps, dt, every, ckpts
-        ctx.nu, ctx.eta, ctx.tape = float(nu), float(eta), tape
+        ctx.nu, ctx.eta, ctx.tape, ctx.token = float(nu), float(eta), tape, token
         return out
 
     @staticmethod
@@ -86,6 +99,11 @@ class _Integrate(torch.autograd.Function):
         for seg in reversed(range(len(ctx.ckpts))):
             n0 = seg * every
             n1 = min(n0 + every, steps)
+            last = seg == len(ctx.ckpts) - 1
+            if last and ctx.tape and ctx.token is not None and dev.tape_token is ctx.token:
+                # the last segment's states are still on the tape from the forward pass
+                dev.adjoint_tape_backward(n1 - n0, dt)
+                continue
             dev.load_mesh_device(ctx.ckpts[seg], wait_torch=False)
             if ctx.tape:
                 # the library keeps the segment's substep states on its own tape

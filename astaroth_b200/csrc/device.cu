@@ -211,9 +211,11 @@ ensure_bfield(Device d)
 static void
 invalidate_tape_graph(Device d)
 {
-    if (d->tape_valid)
-        cudaGraphExecDestroy(d->tape_exec);
-    d->tape_valid = 0;
+    for (int b = 0; b < 2; ++b) {
+        if (d->tape_valid[b])
+            cudaGraphExecDestroy(d->tape_exec[b]);
+        d->tape_valid[b] = 0;
+    }
 }
 
 static void
@@ -440,6 +442,11 @@ acDeviceSwapBuffers(const Device d)
 
 /* ---- uniforms / config ---- */
 
+static_assert(sizeof(AcMeshInfo) == sizeof(int) * NUM_INT_PARAMS + sizeof(int3) * NUM_INT3_PARAMS +
+                                        sizeof(AcReal) * NUM_REAL_PARAMS +
+                                        sizeof(AcReal3) * NUM_REAL3_PARAMS,
+              "AcMeshInfo has no padding (refresh_config compares it bytewise)");
+
 static AcResult
 refresh_config(Device d, const AcMeshInfo& info)
 {
@@ -455,6 +462,10 @@ refresh_config(Device d, const AcMeshInfo& info)
         fprintf(stderr, "astaroth_b200: AC_precision cannot change after acDeviceCreate\n");
         return AC_FAILURE;
     }
+    /* the same parameters again (AcMeshInfo has no padding): the captured
+     * graphs stay valid */
+    if (memcmp(&next, &d->config, sizeof(AcMeshInfo)) == 0)
+        return AC_SUCCESS;
     d->config = next;
     invalidate_graphs(d);
     AC_CUDA_CHECK(cudaSetDevice(d->id));
@@ -1770,11 +1781,13 @@ acDeviceAdjointTapeForward(const Device d, const Stream stream, const int steps,
         d->adj_tape_states = 3 * steps;
     }
     cudaStream_t st = d->streams[stream];
-    /* the recompute is one CUDA graph, kept for the next call with the same
-     * steps, dt, in-block and stream (one per checkpoint segment) */
-    if (!(d->tape_valid && d->tape_steps == steps && d->tape_dt == dt && d->tape_blk == blk &&
-          d->tape_stream == (int)stream)) {
-        invalidate_tape_graph(d);
+    /* the recompute is one CUDA graph per in-block, kept for the next call
+     * with the same steps, dt and stream (one capture per checkpoint length) */
+    if (!(d->tape_valid[blk] && d->tape_steps[blk] == steps && d->tape_dt[blk] == dt &&
+          d->tape_stream[blk] == (int)stream)) {
+        if (d->tape_valid[blk])
+            cudaGraphExecDestroy(d->tape_exec[blk]);
+        d->tape_valid[blk] = 0;
         cudaGraph_t graph;
         AC_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         const cudaError_t rec = record_tape(d, st, steps, dt);
@@ -1783,16 +1796,15 @@ acDeviceAdjointTapeForward(const Device d, const Stream stream, const int steps,
             d->in_idx[q] = blk;
         AC_CUDA_CHECK(rec);
         AC_CUDA_CHECK(end);
-        const cudaError_t inst = cudaGraphInstantiate(&d->tape_exec, graph, 0);
+        const cudaError_t inst = cudaGraphInstantiate(&d->tape_exec[blk], graph, 0);
         cudaGraphDestroy(graph);
         AC_CUDA_CHECK(inst);
-        d->tape_valid  = 1;
-        d->tape_steps  = steps;
-        d->tape_dt     = dt;
-        d->tape_blk    = blk;
-        d->tape_stream = (int)stream;
+        d->tape_valid[blk]  = 1;
+        d->tape_steps[blk]  = steps;
+        d->tape_dt[blk]     = dt;
+        d->tape_stream[blk] = (int)stream;
     }
-    AC_CUDA_CHECK(cudaGraphLaunch(d->tape_exec, st));
+    AC_CUDA_CHECK(cudaGraphLaunch(d->tape_exec[blk], st));
     d->launches += 9ull * steps;
     d->out_set = 0;
     if ((3 * steps) & 1) /* three swaps per step */
@@ -1804,8 +1816,15 @@ extern "C" AcResult
 acDeviceAdjointTapeBackward(const Device d, const Stream stream, const int steps,
                             const AcReal dt)
 {
-    if (!d || !stream_ok(stream) || steps < 1 || !d->adj_lf || d->adj_tape_states < 3 * steps)
+    if (!d || !stream_ok(stream) || steps < 1)
         return AC_FAILURE;
+    if (!d->adj_lf || d->adj_tape_states < 3 * steps) {
+        fprintf(stderr,
+                "astaroth_b200: acDeviceAdjointTapeBackward(%d steps) needs acDeviceLoadAdjoint "
+                "and a tape of %d states (has %d)\n",
+                steps, 3 * steps, d->adj_tape_states);
+        return AC_FAILURE;
+    }
     if (ensure_adjoint(d) != AC_SUCCESS)
         return AC_FAILURE;
     AC_CUDA_CHECK(cudaSetDevice(d->id));

@@ -174,10 +174,11 @@ struct device_s {
     double* bfield;      /* AC_lbfield: B = curl A, 3 arrays of mx*my*mz doubles */
     double* adj_tape;    /* substep input states of a recomputed segment, 8 fields each */
     int adj_tape_states; /* states the tape holds */
-    /* graph of the last acDeviceAdjointTapeForward (steps, dt, in-block, stream) */
-    cudaGraphExec_t tape_exec;
-    int tape_valid, tape_steps, tape_blk, tape_stream;
-    double tape_dt;
+    /* graphs of acDeviceAdjointTapeForward, one per in-block, each kept for
+     * the next call with the same steps, dt and stream */
+    cudaGraphExec_t tape_exec[2];
+    int tape_valid[2], tape_steps[2], tape_stream[2];
+    double tape_dt[2];
     /* acDeviceSetOutput values; bit p of out_set says output p holds one, until
      * the next launch that recomputes the CFL words */
     double outputs[NUM_REAL_OUTPUTS];

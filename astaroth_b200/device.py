@@ -132,6 +132,7 @@ class Device:
         self.info = info
         self._h = capi.Device_p()
         _check(self.lib.acDeviceCreate(device_id, info, C.byref(self._h)), "acDeviceCreate")
+        self.tape_token = None  # see adjoint_tape_forward
         nx, ny, nz = dims(info)
         g = capi.NGHOST
         self.vols = _Vols(Volume(0, 0, 0), Volume(nx + 2 * g, ny + 2 * g, nz + 2 * g),
@@ -329,9 +330,13 @@ class Device:
                                                         self.vols.n1, dt),
                "acDeviceIntegrateSubstepAdjoint")
 
-    def adjoint_tape_forward(self, steps: int, dt: float, stream: int = 0) -> None:
+    def adjoint_tape_forward(self, steps: int, dt: float, stream: int = 0) -> object:
+        """acDeviceAdjointTapeForward; returns a token that stays the device's
+        `tape_token` until the tape is written again."""
         _check(self.lib.acDeviceAdjointTapeForward(self._h, stream, steps, dt),
                "acDeviceAdjointTapeForward")
+        self.tape_token = object()
+        return self.tape_token
 
     def adjoint_tape_backward(self, steps: int, dt: float, stream: int = 0) -> None:
         _check(self.lib.acDeviceAdjointTapeBackward(self._h, stream, steps, dt),
