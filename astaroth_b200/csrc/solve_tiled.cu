@@ -17,6 +17,8 @@
  * evaluate the stencils of lnrho and uu and the continuity and momentum
  * equations, warps 4-7 those of aa and entropy and the induction and entropy
  * equations; the two exchange 11 + 9 values per cell through shared memory
+ * (6 + 9 in FP64, where the magnetic group reads u and forms exp(-lnrho) and
+ * the sound-speed exponential itself)
  * between the halves of the RHS.  This doubles the warps per SM (the plane
  * ring fills the SM's shared memory, so one CTA fits) without extra loads.
  * The per-cell arithmetic is the one of the plain kernel in solve.cu.  Reference:
@@ -296,14 +298,30 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
                     }
                     upwind_terms(up_l, up_u, vd.v, upr);
                 }
+                /* FP64: the magnetic group reads u and computes the two
+                 * exponentials itself, so only entries H2M_GL .. H2M_DIVU cross */
+                constexpr int k0 = sizeof(T) == 8 ? H2M_GL : 0;
+                constexpr int k1 = sizeof(T) == 8 ? H2M_DIVU + 1 : AC_H2M_COUNT;
 #pragma unroll
-                for (int k = 0; k < AC_H2M_COUNT; ++k)
+                for (int k = k0; k < k1; ++k)
                     xh[k * NCELL + cell] = hx.a[k];
             }
             else {
                 scal_derivs(t, VTXBUF_ENTROPY, sc, sd);
                 vec_derivs(t, VTXBUF_AX, sc, vd);
                 mag_prepare(sd, vd, p, mx);
+                if constexpr (sizeof(T) == 8) {
+                    /* the expressions of hydro_prepare, so the bits are the same;
+                     * fewer shared-memory accesses than the exchange (6 per cell),
+                     * for two more exponentials on the FP64 pipe, which has room */
+                    const T lv        = t(VTXBUF_LNRHO, 0, 0, 0);
+                    const T arg       = p.gamma_inv_cp * sd.v + p.gamma_m1 * (lv - p.lnrho0);
+                    hx.a[H2M_E]       = ac_exp(arg);
+                    hx.a[H2M_INV_RHO] = ac_exp(-lv);
+                    hx.a[H2M_U + 0]   = t(VTXBUF_UUX, 0, 0, 0);
+                    hx.a[H2M_U + 1]   = t(VTXBUF_UUY, 0, 0, 0);
+                    hx.a[H2M_U + 2]   = t(VTXBUF_UUZ, 0, 0, 0);
+                }
 #pragma unroll
                 for (int k = 0; k < AC_M2H_COUNT; ++k)
                     xm[k * NCELL + cell] = mx.a[k];
@@ -328,8 +346,10 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
                 val[3] = vd.v[2];
             }
             else {
+                constexpr int k0 = sizeof(T) == 8 ? H2M_GL : 0;
+                constexpr int k1 = sizeof(T) == 8 ? H2M_DIVU + 1 : AC_H2M_COUNT;
 #pragma unroll
-                for (int k = 0; k < AC_H2M_COUNT; ++k)
+                for (int k = k0; k < k1; ++k)
                     hx.a[k] = xh[k * NCELL + cell];
                 mag_rates(sd, vd, mx, hx, p, r);
                 if (cfl) {
