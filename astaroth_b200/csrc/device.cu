@@ -1,5 +1,9 @@
 /*
- * The device object and the acDevice* C ABI (include/astaroth_b200.h).
+ * The device object and the acDevice* C ABI (include/astaroth_b200.h):
+ * creation, configuration, whole-mesh host transfers, the substep and step,
+ * boundary conditions, reductions and the CFL outputs.  Ranges, transfers
+ * between devices, staged loads, plane packing and snapshots are in
+ * device_data.cu; the discrete adjoint is in device_adjoint.cu.
  *
  * Reference: src/core/device.cc (struct device_s :63-74, acDeviceCreate
  * :509-594, acDeviceDestroy :602-630, swaps :635-663, load/store :666-854,
@@ -17,10 +21,8 @@
 #include <stdlib.h>
 #include <string.h>
 
-#include <errno.h>
-#include <sys/stat.h>
-
 #include "internal.h"
+#include "device_impl.h"
 
 static const char* kVersion = "astaroth_b200 0.1 (sm_100a)";
 
@@ -41,69 +43,6 @@ ac_make_geom(const AcMeshInfo& info, const int precision)
     g.pxy        = (long long)g.px * g.my;
     g.cells      = g.pxy * g.mz;
     return g;
-}
-
-/* ---- buffer access ---- */
-
-static size_t
-elem_size(const Device d)
-{
-    return d->precision == 0 ? sizeof(double) : sizeof(float);
-}
-
-static double*
-arr64(const Device d, const int b, const int q)
-{
-    return (double*)d->hi[b] + (size_t)q * d->geom.cells;
-}
-
-static float*
-arr_hi(const Device d, const int b, const int q)
-{
-    return (float*)d->hi[b] + (size_t)q * d->geom.cells;
-}
-
-static float*
-arr_lo(const Device d, const int b, const int q)
-{
-    return d->lo[b] + (size_t)q * d->geom.cells;
-}
-
-static Fields64
-fields64(const Device d)
-{
-    Fields64 f;
-    for (int q = 0; q < AC_NF; ++q) {
-        f.in[q]     = arr64(d, d->in_idx[q], q);
-        f.out[q]    = arr64(d, 1 - d->in_idx[q], q);
-        f.in_lo[q]  = nullptr;
-        f.out_lo[q] = nullptr;
-    }
-    return f;
-}
-
-static Fields32
-fields32(const Device d)
-{
-    Fields32 f;
-    for (int q = 0; q < AC_NF; ++q) {
-        f.in[q]     = arr_hi(d, d->in_idx[q], q);
-        f.out[q]    = arr_hi(d, 1 - d->in_idx[q], q);
-        f.in_lo[q]  = arr_lo(d, d->in_idx[q], q);
-        f.out_lo[q] = arr_lo(d, 1 - d->in_idx[q], q);
-    }
-    return f;
-}
-
-/* The block holding every field's in-buffer (0 or 1), or -1 when single
- * fields were swapped on their own. */
-static int
-in_block_index(const Device d)
-{
-    for (int q = 1; q < AC_NF; ++q)
-        if (d->in_idx[q] != d->in_idx[0])
-            return -1;
-    return d->in_idx[0];
 }
 
 void
@@ -188,12 +127,6 @@ forcing_for_launch(const AcMeshInfo& info, const double dt, PhysConst* pc)
     pc->forcing     = 1;
 }
 
-static bool
-stream_ok(const Stream s)
-{
-    return (int)s >= 0 && (int)s < NUM_STREAMS;
-}
-
 /* The B arrays of AC_lbfield, allocated (zeroed) when the flag is first set;
  * never during a stream capture (every caller is outside one). */
 static cudaError_t
@@ -208,7 +141,7 @@ ensure_bfield(Device d)
     return cudaMemset(d->bfield, 0, bytes);
 }
 
-static void
+void
 invalidate_tape_graph(Device d)
 {
     for (int b = 0; b < 2; ++b) {
@@ -593,26 +526,6 @@ acDeviceGetConfig(const Device d)
 
 /* ---- host <-> device ---- */
 
-static bool
-host_matches(const Device d, const AcMeshInfo& host)
-{
-    AcMeshInfo h = host;
-    if (acHostUpdateParams(&h) != AC_SUCCESS)
-        return false;
-    const int3 m = h.int3_params[AC_mlocal];
-    return m.x == d->geom.mx && m.y == d->geom.my && m.z == d->geom.mz;
-}
-
-/* The result of a whole-mesh transfer from its per-field results: AC_FAILURE
- * if any field failed, else AC_NOT_ALLOCATED if any host field was NULL. */
-static AcResult
-worst(const AcResult a, const AcResult b)
-{
-    if (a == AC_FAILURE || b == AC_FAILURE)
-        return AC_FAILURE;
-    return a == AC_NOT_ALLOCATED || b == AC_NOT_ALLOCATED ? AC_NOT_ALLOCATED : AC_SUCCESS;
-}
-
 extern "C" AcResult
 acDeviceLoadVertexBuffer(const Device d, const Stream stream, const AcMesh host_mesh,
                          const VertexBufferHandle h)
@@ -694,326 +607,6 @@ acDeviceStoreMesh(const Device d, const Stream stream, AcMesh* host_mesh)
     return res;
 }
 
-/* ---- linear ranges between meshes: the reference's *WithOffset family
- * (src/core/device.cc:666-698 and its store and transfer counterparts).
- * num_vertices consecutive values in host-layout linear order (x fastest,
- * rows of mx) move from position src of the source to position dst of the
- * target, into or out of the device's in-buffer.  FP32-compensated devices
- * split/join the range on the fly.  Ranges must lie inside both meshes. ---- */
-
-static bool
-mesh_dims(const AcMeshInfo& info, long long m[3])
-{
-    AcMeshInfo h = info;
-    if (acHostUpdateParams(&h) != AC_SUCCESS)
-        return false;
-    const int3 v = h.int3_params[AC_mlocal];
-    m[0]         = v.x;
-    m[1]         = v.y;
-    m[2]         = v.z;
-    return v.x > 0 && v.y > 0 && v.z > 0;
-}
-
-/* linear index of p in a mesh of dims m, or -1 when p is outside or the n
- * values from it do not fit */
-static long long
-range_start(const int3 p, const long long m[3], const long long n)
-{
-    if (n < 0 || p.x < 0 || p.y < 0 || p.z < 0 || p.x >= m[0] || p.y >= m[1] || p.z >= m[2])
-        return -1;
-    const long long L = p.x + m[0] * (p.y + m[1] * (long long)p.z);
-    return L + n <= m[0] * m[1] * m[2] ? L : -1;
-}
-
-static void
-device_dims(const Device d, long long m[3])
-{
-    m[0] = d->geom.mx;
-    m[1] = d->geom.my;
-    m[2] = d->geom.mz;
-}
-
-extern "C" AcResult
-acDeviceLoadVertexBufferWithOffset(const Device d, const Stream stream, const AcMesh host_mesh,
-                                   const VertexBufferHandle h, const int3 src, const int3 dst,
-                                   const int num_vertices)
-{
-    if (!d || !stream_ok(stream) || (int)h < 0 || h >= NUM_VTXBUF_HANDLES)
-        return AC_FAILURE;
-    if (!host_mesh.vertex_buffer[h])
-        return AC_NOT_ALLOCATED;
-    long long hm[3], dm[3];
-    device_dims(d, dm);
-    if (!mesh_dims(host_mesh.info, hm))
-        return AC_FAILURE;
-    const long long n = num_vertices, s0 = range_start(src, hm, n), d0 = range_start(dst, dm, n);
-    if (s0 < 0 || d0 < 0)
-        return AC_FAILURE;
-    if (n == 0)
-        return AC_SUCCESS;
-    AC_CUDA_CHECK(cudaSetDevice(d->id));
-    const int b       = d->in_idx[h];
-    cudaStream_t st   = d->streams[stream];
-    const double* hp  = host_mesh.vertex_buffer[h] + s0;
-    if (d->precision == 0) {
-        AC_CUDA_CHECK(cudaMemcpyAsync(arr64(d, b, h) + d0, hp, n * sizeof(double),
-                                      cudaMemcpyHostToDevice, st));
-        return AC_SUCCESS;
-    }
-    AC_CUDA_CHECK(cudaMemcpyAsync(d->staging + d0, hp, n * sizeof(double), cudaMemcpyHostToDevice,
-                                  st));
-    AC_CUDA_CHECK(ac_launch_split_range(d->geom, d->staging, arr_hi(d, b, h), arr_lo(d, b, h),
-                                        d0, n, st, &d->launches));
-    AC_CUDA_CHECK(cudaStreamSynchronize(st)); /* the staging field is shared */
-    return AC_SUCCESS;
-}
-
-extern "C" AcResult
-acDeviceLoadMeshWithOffset(const Device d, const Stream stream, const AcMesh host_mesh,
-                           const int3 src, const int3 dst, const int num_vertices)
-{
-    AcResult res = AC_SUCCESS;
-    for (int q = 0; q < AC_NF; ++q)
-        res = worst(res, acDeviceLoadVertexBufferWithOffset(d, stream, host_mesh,
-                                                            (VertexBufferHandle)q, src, dst,
-                                                            num_vertices));
-    return res;
-}
-
-extern "C" AcResult
-acDeviceStoreVertexBufferWithOffset(const Device d, const Stream stream,
-                                    const VertexBufferHandle h, const int3 src, const int3 dst,
-                                    const int num_vertices, AcMesh* host_mesh)
-{
-    if (!d || !host_mesh || !stream_ok(stream) || (int)h < 0 || h >= NUM_VTXBUF_HANDLES)
-        return AC_FAILURE;
-    if (!host_mesh->vertex_buffer[h])
-        return AC_NOT_ALLOCATED;
-    long long hm[3], dm[3];
-    device_dims(d, dm);
-    if (!mesh_dims(host_mesh->info, hm))
-        return AC_FAILURE;
-    const long long n = num_vertices, s0 = range_start(src, dm, n), d0 = range_start(dst, hm, n);
-    if (s0 < 0 || d0 < 0)
-        return AC_FAILURE;
-    if (n == 0)
-        return AC_SUCCESS;
-    AC_CUDA_CHECK(cudaSetDevice(d->id));
-    const int b     = d->in_idx[h];
-    cudaStream_t st = d->streams[stream];
-    double* hp      = host_mesh->vertex_buffer[h] + d0;
-    if (d->precision == 0) {
-        AC_CUDA_CHECK(cudaMemcpyAsync(hp, arr64(d, b, h) + s0, n * sizeof(double),
-                                      cudaMemcpyDeviceToHost, st));
-    }
-    else {
-        AC_CUDA_CHECK(ac_launch_join_range(d->geom, arr_hi(d, b, h), arr_lo(d, b, h), d->staging,
-                                           s0, n, st, &d->launches));
-        AC_CUDA_CHECK(cudaMemcpyAsync(hp, d->staging + s0, n * sizeof(double),
-                                      cudaMemcpyDeviceToHost, st));
-    }
-    AC_CUDA_CHECK(cudaStreamSynchronize(st)); /* the host range is ready on return */
-    return AC_SUCCESS;
-}
-
-extern "C" AcResult
-acDeviceStoreMeshWithOffset(const Device d, const Stream stream, const int3 src, const int3 dst,
-                            const int num_vertices, AcMesh* host_mesh)
-{
-    AcResult res = AC_SUCCESS;
-    for (int q = 0; q < AC_NF; ++q)
-        res = worst(res, acDeviceStoreVertexBufferWithOffset(d, stream, (VertexBufferHandle)q, src,
-                                                             dst, num_vertices, host_mesh));
-    return res;
-}
-
-/* Device to device (the reference's acDeviceTransfer*, device.cc): on the source
- * device's stream, with a peer copy between GPUs.  Both devices must have the
- * same precision. */
-extern "C" AcResult
-acDeviceTransferVertexBufferWithOffset(const Device from, const Stream stream,
-                                       const VertexBufferHandle h, const int3 src, const int3 dst,
-                                       const int num_vertices, Device to)
-{
-    if (!from || !to || !stream_ok(stream) || (int)h < 0 || h >= NUM_VTXBUF_HANDLES ||
-        from->precision != to->precision)
-        return AC_FAILURE;
-    long long fm[3], tm[3];
-    device_dims(from, fm);
-    device_dims(to, tm);
-    const long long n = num_vertices, s0 = range_start(src, fm, n), d0 = range_start(dst, tm, n);
-    if (s0 < 0 || d0 < 0)
-        return AC_FAILURE;
-    if (n == 0)
-        return AC_SUCCESS;
-    AC_CUDA_CHECK(cudaSetDevice(from->id));
-    cudaStream_t st = from->streams[stream];
-    const int fb = from->in_idx[h], tb = to->in_idx[h];
-    if (from->precision == 0) {
-        AC_CUDA_CHECK(cudaMemcpyPeerAsync(arr64(to, tb, h) + d0, to->id, arr64(from, fb, h) + s0,
-                                          from->id, n * sizeof(double), st));
-        return AC_SUCCESS;
-    }
-    /* FP32-compensated: join into the source's staging field, copy the doubles
-     * to the target's staging field, split there */
-    AC_CUDA_CHECK(ac_launch_join_range(from->geom, arr_hi(from, fb, h), arr_lo(from, fb, h),
-                                       from->staging, s0, n, st, &from->launches));
-    AC_CUDA_CHECK(cudaMemcpyPeerAsync(to->staging + d0, to->id, from->staging + s0, from->id,
-                                      n * sizeof(double), st));
-    AC_CUDA_CHECK(cudaStreamSynchronize(st));
-    AC_CUDA_CHECK(cudaSetDevice(to->id));
-    cudaStream_t tst = to->streams[stream];
-    AC_CUDA_CHECK(ac_launch_split_range(to->geom, to->staging, arr_hi(to, tb, h),
-                                        arr_lo(to, tb, h), d0, n, tst, &to->launches));
-    AC_CUDA_CHECK(cudaStreamSynchronize(tst));
-    return AC_SUCCESS;
-}
-
-extern "C" AcResult
-acDeviceTransferMeshWithOffset(const Device from, const Stream stream, const int3 src,
-                               const int3 dst, const int num_vertices, Device to)
-{
-    AcResult res = AC_SUCCESS;
-    for (int q = 0; q < AC_NF; ++q)
-        res = worst(res, acDeviceTransferVertexBufferWithOffset(from, stream, (VertexBufferHandle)q,
-                                                                src, dst, num_vertices, to));
-    return res;
-}
-
-extern "C" AcResult
-acDeviceTransferVertexBuffer(const Device from, const Stream stream, const VertexBufferHandle h,
-                             Device to)
-{
-    if (!from || !to || from->geom.mx != to->geom.mx || from->geom.my != to->geom.my ||
-        from->geom.mz != to->geom.mz)
-        return AC_FAILURE;
-    const long long n = (long long)from->geom.mx * from->geom.my * from->geom.mz;
-    if (n > 0x7fffffffLL)
-        return AC_FAILURE;
-    const int3 o = {0, 0, 0};
-    return acDeviceTransferVertexBufferWithOffset(from, stream, h, o, o, (int)n, to);
-}
-
-extern "C" AcResult
-acDeviceTransferMesh(const Device from, const Stream stream, Device to)
-{
-    AcResult res = AC_SUCCESS;
-    for (int q = 0; q < AC_NF; ++q)
-        res = worst(res, acDeviceTransferVertexBuffer(from, stream, (VertexBufferHandle)q, to));
-    return res;
-}
-
-/* acDeviceUpdate / acDeviceGetLocalConfig (include/astaroth_device.h:217,246):
- * the same as acDeviceLoadMeshInfo / acDeviceGetConfig on one GPU. */
-extern "C" AcResult
-acDeviceUpdate(Device d, const AcMeshInfo info)
-{
-    return acDeviceLoadMeshInfo(d, info);
-}
-
-extern "C" AcMeshInfo
-acDeviceGetLocalConfig(const Device d)
-{
-    return acDeviceGetConfig(d);
-}
-
-/* acDeviceVolumeCopy (include/astaroth_device.h:235, acc-runtime/api/
- * common_kernels.cc:143-155): copies the box min(in_volume, out_volume) from
- * in at in_offset to out at out_offset, both arrays laid out x fastest with
- * their volume's dims.  Unlike the reference, a box that would reach past
- * either array is refused. */
-extern "C" AcResult
-acDeviceVolumeCopy(const Device d, const Stream stream, const AcReal* in, const Volume in_offset,
-                   const Volume in_volume, AcReal* out, const Volume out_offset,
-                   const Volume out_volume)
-{
-    if (!d || !in || !out || !stream_ok(stream))
-        return AC_FAILURE;
-    const Volume nn = {in_volume.x < out_volume.x ? in_volume.x : out_volume.x,
-                       in_volume.y < out_volume.y ? in_volume.y : out_volume.y,
-                       in_volume.z < out_volume.z ? in_volume.z : out_volume.z};
-    if (in_offset.x + nn.x > in_volume.x || in_offset.y + nn.y > in_volume.y ||
-        in_offset.z + nn.z > in_volume.z || out_offset.x + nn.x > out_volume.x ||
-        out_offset.y + nn.y > out_volume.y || out_offset.z + nn.z > out_volume.z)
-        return AC_FAILURE;
-    AC_CUDA_CHECK(cudaSetDevice(d->id));
-    AC_CUDA_CHECK(ac_launch_volume_copy(in, in_offset, in_volume, out, out_offset, out_volume, nn,
-                                        d->streams[stream], &d->launches));
-    return AC_SUCCESS;
-}
-
-/* ---- pipelined loads of whole meshes ----
- * acDeviceLoadMeshStaged copies a host mesh into a device-side stage on
- * `stream` and returns at once; acDeviceCommitStagedMesh makes `stream` wait
- * for that copy and moves the stage into the in-buffer (a device copy, or the
- * hi/lo split of FP32-compensated meshes).  A caller that integrates on one
- * stream and stages the next input on another overlaps the host transfer
- * with the integration; the next staged load waits until the commit has read
- * the stage.  Host buffers must be page-locked for the copy to run
- * asynchronously. */
-static cudaError_t
-ensure_stage(Device d)
-{
-    if (d->stage)
-        return cudaSuccess;
-    const size_t n = (size_t)d->geom.mx * d->geom.my * d->geom.mz;
-    cudaError_t e  = cudaMalloc((void**)&d->stage, AC_NF * n * sizeof(double));
-    if (e != cudaSuccess)
-        return e;
-    e = cudaEventCreateWithFlags(&d->stage_loaded, cudaEventDisableTiming);
-    if (e != cudaSuccess)
-        return e;
-    return cudaEventCreateWithFlags(&d->stage_read, cudaEventDisableTiming);
-}
-
-extern "C" AcResult
-acDeviceLoadMeshStaged(const Device d, const Stream stream, const AcMesh host_mesh)
-{
-    if (!d || !stream_ok(stream))
-        return AC_FAILURE;
-    for (int q = 0; q < AC_NF; ++q)
-        if (!host_mesh.vertex_buffer[q])
-            return AC_NOT_ALLOCATED;
-    if (!host_matches(d, host_mesh.info)) {
-        fprintf(stderr, "astaroth_b200: host mesh dimensions differ from the device's\n");
-        return AC_FAILURE;
-    }
-    AC_CUDA_CHECK(cudaSetDevice(d->id));
-    const bool first = d->stage == nullptr;
-    AC_CUDA_CHECK(ensure_stage(d));
-    cudaStream_t st = d->streams[stream];
-    if (!first) /* the previous commit has read the stage */
-        AC_CUDA_CHECK(cudaStreamWaitEvent(st, d->stage_read, 0));
-    const size_t n = (size_t)d->geom.mx * d->geom.my * d->geom.mz;
-    for (int q = 0; q < AC_NF; ++q)
-        AC_CUDA_CHECK(cudaMemcpyAsync(d->stage + q * n, host_mesh.vertex_buffer[q],
-                                      n * sizeof(double), cudaMemcpyHostToDevice, st));
-    AC_CUDA_CHECK(cudaEventRecord(d->stage_loaded, st));
-    return AC_SUCCESS;
-}
-
-extern "C" AcResult
-acDeviceCommitStagedMesh(const Device d, const Stream stream)
-{
-    if (!d || !stream_ok(stream) || !d->stage)
-        return AC_FAILURE;
-    AC_CUDA_CHECK(cudaSetDevice(d->id));
-    cudaStream_t st = d->streams[stream];
-    AC_CUDA_CHECK(cudaStreamWaitEvent(st, d->stage_loaded, 0));
-    const size_t n = (size_t)d->geom.mx * d->geom.my * d->geom.mz;
-    for (int q = 0; q < AC_NF; ++q) {
-        const int b = d->in_idx[q];
-        if (d->precision == 0)
-            AC_CUDA_CHECK(ac_launch_copy(d->stage + q * n, arr64(d, b, q), (long long)n, st,
-                                         &d->launches));
-        else
-            AC_CUDA_CHECK(ac_launch_split(d->geom, d->stage + q * n, arr_hi(d, b, q),
-                                          arr_lo(d, b, q), st, &d->launches));
-    }
-    AC_CUDA_CHECK(cudaEventRecord(d->stage_read, st));
-    return AC_SUCCESS;
-}
-
 extern "C" AcResult
 acDeviceSetVertexBuffer(const Device d, const Stream stream, const VertexBufferHandle h,
                         const AcReal value)
@@ -1068,13 +661,6 @@ acDeviceResetMesh(const Device d, const Stream stream)
 
 /* ---- integration ---- */
 
-static bool
-is_whole_interior(const Device d, const Volume start, const Volume end)
-{
-    return start.x == NGHOST && start.y == NGHOST && start.z == NGHOST &&
-           end.x == (size_t)(d->geom.nx + NGHOST) && end.y == (size_t)(d->geom.ny + NGHOST) &&
-           end.z == (size_t)(d->geom.nz + NGHOST);
-}
 
 RkCoef
 ac_rk_coef(const int step, const double dt)
@@ -1090,7 +676,7 @@ ac_rk_coef(const int step, const double dt)
     return rk;
 }
 
-static cudaError_t
+cudaError_t
 launch_substep(Device d, cudaStream_t st, const int step, const double dt,
                unsigned long long* launches)
 {
@@ -1154,7 +740,7 @@ launch_substep(Device d, cudaStream_t st, const int step, const double dt,
 }
 
 /* Periodic halo fill of the in-buffer of fields [q0, q0 + nq). */
-static cudaError_t
+cudaError_t
 launch_periodic(Device d, cudaStream_t st, const int q0, const int nq, const Volume start,
                 const Volume end, unsigned long long* launches)
 {
@@ -1579,479 +1165,6 @@ acDeviceSetOutput(const Device d, const AcRealOutputParam param, const AcReal va
         return AC_FAILURE;
     d->outputs[param] = value;
     d->out_set |= 1u << param;
-    return AC_SUCCESS;
-}
-
-/* ---- transfers from and to caller-owned device arrays ---- */
-
-extern "C" AcResult
-acDeviceLoadMeshDevice(const Device d, const Stream stream, const AcReal* const* src)
-{
-    if (!d || !src || !stream_ok(stream))
-        return AC_FAILURE;
-    AC_CUDA_CHECK(cudaSetDevice(d->id));
-    const size_t n = (size_t)d->geom.mx * d->geom.my * d->geom.mz;
-    for (int q = 0; q < AC_NF; ++q) {
-        if (!src[q])
-            return AC_NOT_ALLOCATED;
-        const int b = d->in_idx[q];
-        if (d->precision == 0)
-            AC_CUDA_CHECK(cudaMemcpyAsync(arr64(d, b, q), src[q], n * sizeof(double),
-                                          cudaMemcpyDeviceToDevice, d->streams[stream]));
-        else
-            AC_CUDA_CHECK(ac_launch_split(d->geom, src[q], arr_hi(d, b, q), arr_lo(d, b, q),
-                                          d->streams[stream], &d->launches));
-    }
-    return AC_SUCCESS;
-}
-
-extern "C" AcResult
-acDeviceStoreMeshDevice(const Device d, const Stream stream, AcReal* const* dst)
-{
-    if (!d || !dst || !stream_ok(stream))
-        return AC_FAILURE;
-    AC_CUDA_CHECK(cudaSetDevice(d->id));
-    const size_t n = (size_t)d->geom.mx * d->geom.my * d->geom.mz;
-    for (int q = 0; q < AC_NF; ++q) {
-        if (!dst[q])
-            return AC_NOT_ALLOCATED;
-        const int b = d->in_idx[q];
-        if (d->precision == 0)
-            AC_CUDA_CHECK(cudaMemcpyAsync(dst[q], arr64(d, b, q), n * sizeof(double),
-                                          cudaMemcpyDeviceToDevice, d->streams[stream]));
-        else
-            AC_CUDA_CHECK(ac_launch_join(d->geom, arr_hi(d, b, q), arr_lo(d, b, q), dst[q],
-                                         d->streams[stream], &d->launches));
-    }
-    return AC_SUCCESS;
-}
-
-/* ---- discrete adjoint ---- */
-
-static AcResult
-ensure_adjoint(const Device d)
-{
-    if (d->precision != 0) {
-        fprintf(stderr, "astaroth_b200: the adjoint needs an FP64 device (AC_precision = 0)\n");
-        return AC_FAILURE;
-    }
-    if (d->config.int_params[AC_upwind]) {
-        /* |u| in the upwinding terms has no derivative at u = 0; the reverse
-         * pass covers the equations without them */
-        fprintf(stderr, "astaroth_b200: the adjoint does not cover AC_upwind\n");
-        return AC_FAILURE;
-    }
-    if (d->adj_lf)
-        return AC_SUCCESS;
-    const size_t fb = (size_t)d->geom.cells * sizeof(double);
-    AC_CUDA_CHECK(cudaMalloc((void**)&d->adj_lf, AC_NF * fb));
-    AC_CUDA_CHECK(cudaMalloc((void**)&d->adj_lw, AC_NF * fb));
-    AC_CUDA_CHECK(cudaMalloc((void**)&d->adj_mu, AC_MU_COUNT * fb));
-    AC_CUDA_CHECK(cudaMalloc((void**)&d->adj_pgrad, 2 * sizeof(double)));
-    AC_CUDA_CHECK(cudaMemset(d->adj_mu, 0, AC_MU_COUNT * fb));
-    return AC_SUCCESS;
-}
-
-extern "C" AcResult
-acDeviceLoadAdjoint(const Device d, const Stream stream, const AcReal* const* lam_f)
-{
-    if (!d || !stream_ok(stream))
-        return AC_FAILURE;
-    AC_CUDA_CHECK(cudaSetDevice(d->id));
-    if (ensure_adjoint(d) != AC_SUCCESS)
-        return AC_FAILURE;
-    cudaStream_t st = d->streams[stream];
-    const size_t fb = (size_t)d->geom.cells * sizeof(double);
-    for (int q = 0; q < AC_NF; ++q) {
-        if (lam_f && lam_f[q])
-            AC_CUDA_CHECK(cudaMemcpyAsync(d->adj_lf + (size_t)q * d->geom.cells, lam_f[q], fb,
-                                          cudaMemcpyDeviceToDevice, st));
-        else
-            AC_CUDA_CHECK(cudaMemsetAsync(d->adj_lf + (size_t)q * d->geom.cells, 0, fb, st));
-    }
-    AC_CUDA_CHECK(cudaMemsetAsync(d->adj_lw, 0, AC_NF * fb, st));
-    AC_CUDA_CHECK(cudaMemsetAsync(d->adj_pgrad, 0, 2 * sizeof(double), st));
-    return AC_SUCCESS;
-}
-
-extern "C" AcResult
-acDeviceStoreAdjoint(const Device d, const Stream stream, AcReal* const* lam_f)
-{
-    if (!d || !lam_f || !stream_ok(stream) || !d->adj_lf)
-        return AC_FAILURE;
-    AC_CUDA_CHECK(cudaSetDevice(d->id));
-    const size_t fb = (size_t)d->geom.cells * sizeof(double);
-    for (int q = 0; q < AC_NF; ++q)
-        if (lam_f[q])
-            AC_CUDA_CHECK(cudaMemcpyAsync(lam_f[q], d->adj_lf + (size_t)q * d->geom.cells, fb,
-                                          cudaMemcpyDeviceToDevice, d->streams[stream]));
-    return AC_SUCCESS;
-}
-
-/* One adjoint substep about the state `state` (8 fields at q * cells, halos
- * filled), or about the in-buffers when state is NULL. */
-static cudaError_t
-launch_adjoint(const Device d, cudaStream_t st, const int step, const double dt,
-               const double* state)
-{
-    StencilCoef sc;
-    PhysConst pc;
-    ac_make_stencil(d->config, &sc);
-    ac_make_phys(d->config, &pc);
-    AdjointFields a;
-    for (int q = 0; q < AC_NF; ++q) {
-        a.f[q]  = state ? state + (size_t)q * d->geom.cells : arr64(d, d->in_idx[q], q);
-        a.lf[q] = d->adj_lf + (size_t)q * d->geom.cells;
-        a.lw[q] = d->adj_lw + (size_t)q * d->geom.cells;
-    }
-    for (int m = 0; m < AC_MU_COUNT; ++m)
-        a.mu[m] = d->adj_mu + (size_t)m * d->geom.cells;
-    const double alpha[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
-    const double beta[3]  = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
-    return ac_launch_adjoint_substep(d->geom, a, sc, pc, alpha[step], beta[step], dt,
-                                     d->adj_pgrad, st, &d->launches);
-}
-
-extern "C" AcResult
-acDeviceIntegrateSubstepAdjoint(const Device d, const Stream stream, const int step_number,
-                                const Volume start, const Volume end, const AcReal dt)
-{
-    if (!d || !stream_ok(stream) || step_number < 0 || step_number > 2 || !d->adj_lf)
-        return AC_FAILURE;
-    if (ensure_adjoint(d) != AC_SUCCESS)
-        return AC_FAILURE;
-    if (!is_whole_interior(d, start, end)) {
-        fprintf(stderr, "astaroth_b200: acDeviceIntegrateSubstepAdjoint needs the whole interior\n");
-        return AC_FAILURE;
-    }
-    AC_CUDA_CHECK(cudaSetDevice(d->id));
-    AC_CUDA_CHECK(launch_adjoint(d, d->streams[stream], step_number, dt, NULL));
-    return AC_SUCCESS;
-}
-
-/* The launches of a tape recompute: per substep, halo fill, copy of the
- * in-block to the tape, substep, swap. */
-static cudaError_t
-record_tape(Device d, cudaStream_t st, const int steps, const double dt)
-{
-    const size_t state_elems = (size_t)AC_NF * d->geom.cells;
-    const Volume m0          = {0, 0, 0};
-    const Volume m1          = {(size_t)d->geom.mx, (size_t)d->geom.my, (size_t)d->geom.mz};
-    for (int n = 0; n < steps; ++n)
-        for (int s = 0; s < 3; ++s) {
-            cudaError_t e = launch_periodic(d, st, 0, AC_NF, m0, m1, NULL);
-            if (e != cudaSuccess)
-                return e;
-            /* the 8 in-buffers are one contiguous block: one copy per state */
-            e = ac_launch_copy(arr64(d, d->in_idx[0], 0),
-                               d->adj_tape + (size_t)(3 * n + s) * state_elems,
-                               (long long)state_elems, st, NULL);
-            if (e != cudaSuccess)
-                return e;
-            e = launch_substep(d, st, s, dt, NULL);
-            if (e != cudaSuccess)
-                return e;
-            acDeviceSwapBuffers(d);
-        }
-    return cudaSuccess;
-}
-
-extern "C" AcResult
-acDeviceAdjointTapeForward(const Device d, const Stream stream, const int steps, const AcReal dt)
-{
-    if (!d || !stream_ok(stream) || steps < 1)
-        return AC_FAILURE;
-    const int blk = in_block_index(d);
-    if (blk < 0) {
-        fprintf(stderr, "astaroth_b200: the tape needs every field's in-buffer in one block\n");
-        return AC_FAILURE;
-    }
-    AC_CUDA_CHECK(cudaSetDevice(d->id));
-    if (ensure_adjoint(d) != AC_SUCCESS)
-        return AC_FAILURE;
-    const size_t state_elems = (size_t)AC_NF * d->geom.cells;
-    if (d->adj_tape_states < 3 * steps) {
-        AC_CUDA_CHECK(cudaDeviceSynchronize());
-        invalidate_tape_graph(d);
-        cudaFree(d->adj_tape);
-        d->adj_tape        = NULL;
-        d->adj_tape_states = 0;
-        AC_CUDA_CHECK(cudaMalloc((void**)&d->adj_tape, 3 * (size_t)steps * state_elems *
-                                                           sizeof(double)));
-        d->adj_tape_states = 3 * steps;
-    }
-    cudaStream_t st = d->streams[stream];
-    /* the recompute is one CUDA graph per in-block, kept for the next call
-     * with the same steps, dt and stream (one capture per checkpoint length) */
-    if (!(d->tape_valid[blk] && d->tape_steps[blk] == steps && d->tape_dt[blk] == dt &&
-          d->tape_stream[blk] == (int)stream)) {
-        if (d->tape_valid[blk])
-            cudaGraphExecDestroy(d->tape_exec[blk]);
-        d->tape_valid[blk] = 0;
-        cudaGraph_t graph;
-        AC_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-        const cudaError_t rec = record_tape(d, st, steps, dt);
-        const cudaError_t end = cudaStreamEndCapture(st, &graph);
-        for (int q = 0; q < AC_NF; ++q) /* undo the capture's swaps */
-            d->in_idx[q] = blk;
-        AC_CUDA_CHECK(rec);
-        AC_CUDA_CHECK(end);
-        const cudaError_t inst = cudaGraphInstantiate(&d->tape_exec[blk], graph, 0);
-        cudaGraphDestroy(graph);
-        AC_CUDA_CHECK(inst);
-        d->tape_valid[blk]  = 1;
-        d->tape_steps[blk]  = steps;
-        d->tape_dt[blk]     = dt;
-        d->tape_stream[blk] = (int)stream;
-    }
-    AC_CUDA_CHECK(cudaGraphLaunch(d->tape_exec[blk], st));
-    d->launches += 9ull * steps;
-    d->out_set = 0;
-    if ((3 * steps) & 1) /* three swaps per step */
-        acDeviceSwapBuffers(d);
-    return AC_SUCCESS;
-}
-
-extern "C" AcResult
-acDeviceAdjointTapeBackward(const Device d, const Stream stream, const int steps,
-                            const AcReal dt)
-{
-    if (!d || !stream_ok(stream) || steps < 1)
-        return AC_FAILURE;
-    if (!d->adj_lf || d->adj_tape_states < 3 * steps) {
-        fprintf(stderr,
-                "astaroth_b200: acDeviceAdjointTapeBackward(%d steps) needs acDeviceLoadAdjoint "
-                "and a tape of %d states (has %d)\n",
-                steps, 3 * steps, d->adj_tape_states);
-        return AC_FAILURE;
-    }
-    if (ensure_adjoint(d) != AC_SUCCESS)
-        return AC_FAILURE;
-    AC_CUDA_CHECK(cudaSetDevice(d->id));
-    cudaStream_t st             = d->streams[stream];
-    const size_t state_elems    = (size_t)AC_NF * d->geom.cells;
-    for (int n = steps - 1; n >= 0; --n)
-        for (int s = 2; s >= 0; --s)
-            AC_CUDA_CHECK(launch_adjoint(d, st, s, dt,
-                                         d->adj_tape + (size_t)(3 * n + s) * state_elems));
-    return AC_SUCCESS;
-}
-
-extern "C" AcResult
-acDeviceGetParamAdjoints(const Device d, AcReal* nu_bar, AcReal* eta_bar)
-{
-    if (!d || !nu_bar || !eta_bar || !d->adj_pgrad)
-        return AC_FAILURE;
-    AC_CUDA_CHECK(cudaSetDevice(d->id));
-    for (int s = 0; s < NUM_STREAMS; ++s)
-        AC_CUDA_CHECK(cudaStreamSynchronize(d->streams[s]));
-    double v[2];
-    AC_CUDA_CHECK(cudaMemcpy(v, d->adj_pgrad, sizeof(v), cudaMemcpyDeviceToHost));
-    *nu_bar  = v[0];
-    *eta_bar = v[1];
-    return AC_SUCCESS;
-}
-
-/* ---- whole-plane copies for a z-slab decomposition ----
- * The halo exchange of the reference's grid layer packs boundary slabs into
- * buffers and unpacks them into the neighbours' ghost zones
- * (src/core/kernels/packing.cuh:59-470, src/core/task.cc:1933-1993).  With a
- * decomposition along z only, a z halo is a run of whole xy planes, contiguous
- * in every field array, so packing is one copy per array: the buffer holds, for
- * each array (the 8 value arrays, then the 8 compensation arrays of FP32
- * meshes), `nplanes` planes of px*my elements. */
-static bool
-planes_ok(const Device d, const int z0, const int nplanes)
-{
-    return d && nplanes > 0 && z0 >= 0 && z0 + nplanes <= d->geom.mz;
-}
-
-static int
-plane_arrays(const Device d)
-{
-    return d->precision == 0 ? AC_NF : 2 * AC_NF;
-}
-
-extern "C" size_t
-acDevicePlaneBytes(const Device d)
-{
-    return d ? (size_t)d->geom.pxy * elem_size(d) * plane_arrays(d) : 0;
-}
-
-static AcResult
-copy_planes(const Device d, const Stream stream, const int z0, const int nplanes, char* buffer,
-            const bool pack)
-{
-    if (!planes_ok(d, z0, nplanes) || !buffer || !stream_ok(stream))
-        return AC_FAILURE;
-    AC_CUDA_CHECK(cudaSetDevice(d->id));
-    const size_t es = elem_size(d);
-    void* arrays[2 * AC_NF];
-    for (int a = 0; a < plane_arrays(d); ++a) {
-        const int q = a % AC_NF;
-        arrays[a]   = a < AC_NF ? (void*)((char*)d->hi[d->in_idx[q]] + (size_t)q * d->geom.cells * es)
-                                : (void*)arr_lo(d, d->in_idx[q], q);
-    }
-    /* one launch for all arrays (the buffer holds array a at a * bytes) */
-    AC_CUDA_CHECK(ac_launch_planes(arrays, plane_arrays(d), (long long)z0 * d->geom.pxy * es,
-                                   (long long)nplanes * d->geom.pxy * es, buffer, pack,
-                                   d->streams[stream], &d->launches));
-    return AC_SUCCESS;
-}
-
-extern "C" AcResult
-acDevicePackPlanes(const Device d, const Stream stream, const int z0, const int nplanes,
-                   void* buffer)
-{
-    return copy_planes(d, stream, z0, nplanes, (char*)buffer, true);
-}
-
-extern "C" AcResult
-acDeviceUnpackPlanes(const Device d, const Stream stream, const int z0, const int nplanes,
-                     const void* buffer)
-{
-    return copy_planes(d, stream, z0, nplanes, (char*)buffer, false);
-}
-
-/* ---- snapshots of the computational domain: src/core/grid.cc:3792-3935 ----
- * One raw file per field holding the interior nx*ny*nz values (x fastest):
- * <dir>/<field name>-<label>.mesh, or with `segmented`,
- * <dir>/<field name>-segment-<ox>-<oy>-<oz>-<label>.mesh where (ox, oy, oz) is
- * AC_multigpu_offset ((0, 0, 0) on one GPU), the names the reference's grid
- * layer writes without and with distributed I/O.  FP32-compensated meshes are
- * written as the double values hi + lo. */
-static const char* const kSnapNames[NUM_VTXBUF_HANDLES] = {
-    "VTXBUF_LNRHO", "VTXBUF_UUX", "VTXBUF_UUY", "VTXBUF_UUZ",
-    "VTXBUF_AX",    "VTXBUF_AY",  "VTXBUF_AZ",  "VTXBUF_ENTROPY"};
-
-static bool
-snapshot_path(const Device d, const char* dir, const char* label, const int segmented,
-              const int q, char* out, const size_t len)
-{
-    const int3 o = d->config.int3_params[AC_multigpu_offset];
-    const int n  = segmented ? snprintf(out, len, "%s/%s-segment-%d-%d-%d-%s.mesh", dir,
-                                        kSnapNames[q], o.x, o.y, o.z, label)
-                             : snprintf(out, len, "%s/%s-%s.mesh", dir, kSnapNames[q], label);
-    return n >= 0 && (size_t)n < len;
-}
-
-extern "C" AcResult
-acDeviceWriteMeshToDisk(const Device d, const char* dir, const char* label, const int segmented)
-{
-    if (!d || !dir || !label)
-        return AC_FAILURE;
-    if (mkdir(dir, 0755) != 0 && errno != EEXIST) {
-        fprintf(stderr, "astaroth_b200: cannot create %s\n", dir);
-        return AC_FAILURE;
-    }
-    const Geom& g   = d->geom;
-    const size_t nm = (size_t)g.mx * g.my * g.mz;
-    double* buf     = (double*)malloc(nm * sizeof(double));
-    if (!buf)
-        return AC_FAILURE;
-    AcResult res = AC_SUCCESS;
-    for (int q = 0; q < AC_NF && res == AC_SUCCESS; ++q) {
-        AcMesh m;
-        memset(&m, 0, sizeof(m));
-        m.info            = d->config;
-        m.vertex_buffer[q] = buf;
-        res = acDeviceStoreVertexBuffer(d, STREAM_DEFAULT, (VertexBufferHandle)q, &m);
-        if (res != AC_SUCCESS)
-            break;
-        char path[4096];
-        FILE* fp = NULL;
-        if (!snapshot_path(d, dir, label, segmented, q, path, sizeof(path)) ||
-            !(fp = fopen(path, "wb"))) {
-            res = AC_FAILURE;
-            break;
-        }
-        for (int k = 0; k < g.nz && res == AC_SUCCESS; ++k)
-            for (int j = 0; j < g.ny; ++j) {
-                const double* row = buf + NGHOST + (size_t)g.mx * ((j + NGHOST) +
-                                                                  (size_t)g.my * (k + NGHOST));
-                if (fwrite(row, sizeof(double), g.nx, fp) != (size_t)g.nx) {
-                    res = AC_FAILURE;
-                    break;
-                }
-            }
-        if (fclose(fp) != 0)
-            res = AC_FAILURE;
-    }
-    free(buf);
-    return res;
-}
-
-extern "C" AcResult
-acDeviceReadMeshFromDisk(const Device d, const char* dir, const char* label, const int segmented)
-{
-    if (!d || !dir || !label)
-        return AC_FAILURE;
-    const Geom& g   = d->geom;
-    const size_t nm = (size_t)g.mx * g.my * g.mz;
-    double* buf     = (double*)calloc(nm, sizeof(double));
-    if (!buf)
-        return AC_FAILURE;
-    AcResult res = AC_SUCCESS;
-    for (int q = 0; q < AC_NF && res == AC_SUCCESS; ++q) {
-        char path[4096];
-        FILE* fp = NULL;
-        if (!snapshot_path(d, dir, label, segmented, q, path, sizeof(path)) ||
-            !(fp = fopen(path, "rb"))) {
-            fprintf(stderr, "astaroth_b200: cannot open snapshot field %d in %s\n", q, dir);
-            res = AC_FAILURE;
-            break;
-        }
-        for (int k = 0; k < g.nz && res == AC_SUCCESS; ++k)
-            for (int j = 0; j < g.ny; ++j) {
-                double* row = buf + NGHOST + (size_t)g.mx * ((j + NGHOST) +
-                                                            (size_t)g.my * (k + NGHOST));
-                if (fread(row, sizeof(double), g.nx, fp) != (size_t)g.nx) {
-                    res = AC_FAILURE;
-                    break;
-                }
-            }
-        /* the file must hold exactly the interior */
-        if (res == AC_SUCCESS && fgetc(fp) != EOF)
-            res = AC_FAILURE;
-        fclose(fp);
-        if (res != AC_SUCCESS)
-            break;
-        AcMesh m;
-        memset(&m, 0, sizeof(m));
-        m.info            = d->config;
-        m.vertex_buffer[q] = buf;
-        res = acDeviceLoadVertexBuffer(d, STREAM_DEFAULT, m, (VertexBufferHandle)q);
-        if (res == AC_SUCCESS && cudaStreamSynchronize(d->streams[STREAM_DEFAULT]) != cudaSuccess)
-            res = AC_FAILURE;
-    }
-    free(buf);
-    if (res != AC_SUCCESS)
-        return res;
-    /* the halos follow from the interior by the periodic fill */
-    const Volume m0 = {0, 0, 0};
-    const Volume m1 = {(size_t)g.mx, (size_t)g.my, (size_t)g.mz};
-    res = acDevicePeriodicBoundconds(d, STREAM_DEFAULT, m0, m1);
-    if (res == AC_SUCCESS)
-        res = acDeviceSynchronizeStream(d, STREAM_DEFAULT);
-    return res;
-}
-
-extern "C" AcResult
-acDeviceStoreBfield(const Device d, const Stream stream, AcReal* bx, AcReal* by, AcReal* bz)
-{
-    if (!d || !stream_ok(stream) || !bx || !by || !bz)
-        return AC_FAILURE;
-    if (!d->config.int_params[AC_lbfield] || !d->bfield) {
-        fprintf(stderr, "astaroth_b200: acDeviceStoreBfield needs AC_lbfield\n");
-        return AC_FAILURE;
-    }
-    AC_CUDA_CHECK(cudaSetDevice(d->id));
-    const size_t nm = (size_t)d->geom.mx * d->geom.my * d->geom.mz;
-    AcReal* out[3]  = {bx, by, bz};
-    for (int c = 0; c < 3; ++c)
-        AC_CUDA_CHECK(cudaMemcpyAsync(out[c], d->bfield + c * nm, nm * sizeof(double),
-                                      cudaMemcpyDeviceToHost, d->streams[stream]));
-    AC_CUDA_CHECK(cudaStreamSynchronize(d->streams[stream]));
     return AC_SUCCESS;
 }
 
