@@ -160,6 +160,34 @@ scal_derivs(const Taps<T>& t, const int q, const StencilT<T>& sc, ScalD<T>& o)
             d2_sides<1>(t, q, sc.d2[1]) + d2_sides<2>(t, q, sc.d2[2]);
 }
 
+/* scal_derivs with the z-line of the field (planes z-3 .. z+3 at this
+ * thread's cell) from registers */
+template <typename T>
+__device__ __forceinline__ void
+scal_derivs_zq(const Taps<T>& t, const int q, const StencilT<T>& sc, const T zq[7], ScalD<T>& o)
+{
+    o.v    = zq[3];
+    o.g[0] = d1<0>(t, q, sc.d1[0]);
+    o.g[1] = d1<1>(t, q, sc.d1[1]);
+    {
+        const T* c = sc.d1[2];
+        T r = c[0] * (zq[4] - zq[2]);
+        r   = fma(c[1], zq[5] - zq[1], r);
+        r   = fma(c[2], zq[6] - zq[0], r);
+        o.g[2] = r;
+    }
+    T s2;
+    {
+        const T* d = sc.d2[2];
+        T r = d[1] * (zq[4] + zq[2]);
+        r   = fma(d[2], zq[5] + zq[1], r);
+        r   = fma(d[3], zq[6] + zq[0], r);
+        s2 = r;
+    }
+    o.lap  = (sc.d2[0][0] + sc.d2[1][0] + sc.d2[2][0]) * o.v + d2_sides<0>(t, q, sc.d2[0]) +
+            d2_sides<1>(t, q, sc.d2[1]) + s2;
+}
+
 template <typename T>
 __device__ __forceinline__ void
 vec_derivs(const Taps<T>& t, const int q0, const StencilT<T>& sc, VecD<T>& o)
@@ -242,6 +270,11 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
     bool ok    = true;
     int waited = pfirst - 1;
     T cm[3]    = {0, 0, 0}; /* CFL maxima of this thread (substep 2 only) */
+    /* the group's scalar field (lnrho or entropy) at this cell, planes z-3 ..
+     * z+3, shifted by one plane per step: its z taps come from registers, 6
+     * shared-memory loads fewer per cell and field */
+    T zq[7];
+    const int qs = group == 0 ? VTXBUF_LNRHO : VTXBUF_ENTROPY;
 
     for (int z = z0; z < z1; ++z) {
         const long long idx = geom_idx(g, x + NGHOST, y + NGHOST, z + NGHOST);
@@ -273,6 +306,17 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
 #pragma unroll
         for (int k = 0; k < 7; ++k)
             t.off[k] = ((z - NGHOST + k - pfirst) & (RING - 1)) * L::SLOT + cell_off;
+        if (z == z0) {
+#pragma unroll
+            for (int k = 0; k < 7; ++k)
+                zq[k] = t(qs, 0, 0, k - 3);
+        }
+        else {
+#pragma unroll
+            for (int k = 0; k < 6; ++k)
+                zq[k] = zq[k + 1];
+            zq[6] = t(qs, 0, 0, 3);
+        }
 
         ScalD<T> sd;
         VecD<T> vd;
@@ -282,7 +326,7 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
         T upr[4] = {0, 0, 0, 0}; /* upwinding terms of the hydro rates (UPWD) */
         if (active) {
             if (group == 0) {
-                scal_derivs(t, VTXBUF_LNRHO, sc, sd);
+                scal_derivs_zq(t, VTXBUF_LNRHO, sc, zq, sd);
                 vec_derivs(t, VTXBUF_UUX, sc, vd);
                 hydro_prepare(sd, t(VTXBUF_ENTROPY, 0, 0, 0), vd, p, hx, st);
                 if constexpr (UPWD) {
@@ -307,7 +351,7 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
                     xh[k * NCELL + cell] = hx.a[k];
             }
             else {
-                scal_derivs(t, VTXBUF_ENTROPY, sc, sd);
+                scal_derivs_zq(t, VTXBUF_ENTROPY, sc, zq, sd);
                 vec_derivs(t, VTXBUF_AX, sc, vd);
                 mag_prepare(sd, vd, p, mx);
                 if constexpr (sizeof(T) == 8) {
