@@ -47,6 +47,21 @@ def test_slabs_equal_one_device(shape, slabs, precision):
     assert np.array_equal(_interior(got), _interior(_device(info, f, 3)))
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_slabs_with_upwinding(precision):
+    """The upwinding terms (AC_upwind) are per-cell stencils too: slabs give the
+    bits of one device."""
+    info = make_info((40, 36, 30), precision=precision, upwind=1)
+    f = seeded_mesh(info, 85, sigma_uu=1e-2)
+    with Grid(info, slabs=3) as g:
+        g.load_mesh(f)
+        for _ in range(2):
+            g.integrate_step(DT)
+        g.synchronize()
+        got = g.store_mesh()
+    assert np.array_equal(_interior(got), _interior(_device(info, f, 2)))
+
+
 def test_reductions_and_timestep():
     info = make_info((40, 36, 30))
     f = seeded_mesh(info, 82, sigma_uu=1e-2)
