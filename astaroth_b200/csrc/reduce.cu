@@ -12,6 +12,9 @@
  * result is the correctly rounded sum up to the map's own rounding; the
  * order is fixed by the grid, so repeated calls give identical bits.
  */
+#include <climits>
+#include <mutex>
+
 #include "internal.h"
 
 namespace {
@@ -278,6 +281,7 @@ static __device__ __align__(256) double g_noalloc_scratch[2 * kNoAllocMaxBlocks 
 
 constexpr int kMaxDevicesNoAlloc = 64;
 double* g_noalloc_ptr[kMaxDevicesNoAlloc]; /* device address of the array, per device */
+std::mutex g_noalloc_mutex;                /* guards the one-time fill of g_noalloc_ptr */
 
 } // namespace
 
@@ -288,6 +292,15 @@ acReduceNoAlloc(const AcReal* const* fields, const int nfields, const int nx, co
 {
     if (!fields || !result || nx <= 0 || ny <= 0 || nz <= 0) {
         fprintf(stderr, "acReduceNoAlloc: null pointer or empty mesh\n");
+        return AC_FAILURE;
+    }
+    /* the padded extents n + 6 must fit an int (the kernel's row indices) */
+    if (nx > INT_MAX - 2 * NGHOST || ny > INT_MAX - 2 * NGHOST || nz > INT_MAX - 2 * NGHOST) {
+        fprintf(stderr, "acReduceNoAlloc: mesh extent too large (%d, %d, %d)\n", nx, ny, nz);
+        return AC_FAILURE;
+    }
+    if (blocks < 0) {
+        fprintf(stderr, "acReduceNoAlloc: negative block count %d\n", blocks);
         return AC_FAILURE;
     }
     if (nfields != 1 && nfields != 3 && nfields != 4) {
@@ -342,12 +355,16 @@ acReduceNoAlloc(const AcReal* const* fields, const int nfields, const int nx, co
                 kMaxDevicesNoAlloc);
         return AC_FAILURE;
     }
-    if (!g_noalloc_ptr[dev]) {
-        void* p = nullptr;
-        AC_CUDA_CHECK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        g_noalloc_ptr[dev] = (double*)p;
+    double* partials = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_ptr[dev]) {
+            void* p = nullptr;
+            AC_CUDA_CHECK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+            g_noalloc_ptr[dev] = (double*)p;
+        }
+        partials = g_noalloc_ptr[dev];
     }
-    double* partials      = g_noalloc_ptr[dev];
     unsigned int* counter = (unsigned int*)(partials + 2 * kNoAllocMaxBlocks);
     cudaStream_t st       = (cudaStream_t)stream;
 

@@ -558,3 +558,64 @@ oracle_reduce(const double* const* f, const int nx, const int ny, const int nz, 
     }
     return (double)res;
 }
+
+/* ---------------------------------------------------------------------------
+ * Seeded initial condition of the benchmark workloads, for callers of the
+ * oracle that must not load the product library (the CPU baseline).  The
+ * reference has no seeded Gaussian initial condition (its acHostMeshRandomize
+ * is rand()/RAND_MAX, src/core/astaroth.cc:383-400); this is the project's
+ * counter-based definition: splitmix64 of (seed, field, cell index), a 53-bit
+ * uniform, and Box-Muller for the Gaussian fields.  lnrho and entropy ~
+ * U(-amp, amp); uu ~ N(0, sigma_uu^2); aa ~ N(0, sigma_aa^2); every cell of
+ * the (nx+6)(ny+6)(nz+6) arrays, halos included.  The tests check its bytes
+ * against the input hashes of the golden vectors.
+ * ------------------------------------------------------------------------- */
+static inline unsigned long long
+sm64(unsigned long long x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+static inline double
+unit53(const unsigned long long x)
+{
+    return (double)(x >> 11) * (1.0 / 9007199254740992.0);
+}
+
+int
+oracle_seeded_mesh(double* const* f, const int nx, const int ny, const int nz,
+                   const unsigned long long seed, const double amp_scalar, const double sigma_uu,
+                   const double sigma_aa)
+{
+    const Dims d  = mkdims(nx, ny, nz);
+    const size_t n = (size_t)d.mx * (size_t)d.my * (size_t)d.mz;
+    const unsigned long long base =
+        sm64(seed * 0xD1B54A32D192ED03ull + 0x5851F42D4C957F2Dull);
+    const double two_pi = 6.283185307179586476925286766559;
+    for (int w = 0; w < NFIELDS; ++w) {
+        double* a = f[w];
+        if (!a)
+            continue;
+        const int gaussian = w >= UUX && w <= AZ;
+        const double sigma = w <= UUZ ? sigma_uu : sigma_aa;
+        const unsigned long long fbase =
+            base + (unsigned long long)w * 0x9E3779B97F4A7C15ull * 2ull * (unsigned long long)n;
+#pragma omp parallel for schedule(static)
+        for (long long idx = 0; idx < (long long)n; ++idx) {
+            const unsigned long long c = fbase + 2ull * (unsigned long long)idx;
+            const unsigned long long r1 = sm64(c);
+            if (!gaussian) {
+                a[idx] = amp_scalar * (2.0 * unit53(r1) - 1.0);
+            }
+            else {
+                const double u = 1.0 - unit53(r1); /* (0, 1] */
+                const double v = unit53(sm64(c + 1ull));
+                a[idx]         = sigma * sqrt(-2.0 * log(u)) * cos(two_pi * v);
+            }
+        }
+    }
+    return 0;
+}

@@ -27,7 +27,14 @@ REF_UPWD_LIB = HERE / "_ref" / "libastaroth_ref_upwd.so"
 REF_FORCING_LIB = HERE / "_ref" / "libastaroth_ref_forcing.so"
 _PATHS = {"port": PORT_LIB, "reference": REF_LIB, "reference_upwd": REF_UPWD_LIB,
           "reference_forcing": REF_FORCING_LIB}
-REF_SRC = Path(os.environ.get("AC_REFERENCE", "/root/reference"))
+# The reference tree: $AC_REFERENCE, else a checkout named "reference" beside
+# this repository.  Only the reference model build (_ref/) needs it.
+REF_SRC = Path(os.environ.get("AC_REFERENCE", str(HERE.parent.parent / "reference")))
+
+# Physics of the benchmark workloads (the reference's config/astaroth.conf
+# values where the workloads give none): nu = eta = 5e-3, cs = 1, gamma = 5/3.
+BENCH_PARAMS = dict(nu_visc=5e-3, eta=5e-3, cs_sound=1.0, gamma=5.0 / 3.0, cp_sound=1.0,
+                    lnT0=1.2, lnrho0=1.3, mu0=1.4, zeta=0.01, K_heatcond=1e-3)
 
 RTYPE_NAMES = ["RTYPE_MAX", "RTYPE_MIN", "RTYPE_SUM", "RTYPE_RMS", "RTYPE_RMS_EXP",
                "RTYPE_ALFVEN_MAX", "RTYPE_ALFVEN_MIN", "RTYPE_ALFVEN_RMS"]
@@ -91,6 +98,9 @@ def lib(kind: str = "port") -> C.CDLL:
     f.restype, f.argtypes = C.c_double, [pp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
                                          C.c_int, C.c_int, C.c_int, C.c_int]
     if kind == "port":
+        L.oracle_seeded_mesh.restype = C.c_int
+        L.oracle_seeded_mesh.argtypes = [pp, C.c_int, C.c_int, C.c_int, C.c_ulonglong,
+                                         C.c_double, C.c_double, C.c_double]
         L.oracle_rates.restype = C.c_int
         L.oracle_rates.argtypes = [pp, C.c_int, C.c_int, C.c_int, C.POINTER(OracleParams), pp]
     else:
@@ -100,6 +110,29 @@ def lib(kind: str = "port") -> C.CDLL:
         L.ref_get_error.argtypes = [C.c_double, C.c_double, C.POINTER(C.c_longdouble)]
     _libs[kind] = L
     return L
+
+
+def box_params(n, **over) -> dict:
+    """Oracle params of an n^3 (or (nx, ny, nz)) periodic box [0, 2 pi)^3 with
+    the benchmark physics, overridden by keyword."""
+    nx, ny, nz = (n, n, n) if np.isscalar(n) else n
+    two_pi = 6.283185307179586476925286766559
+    p = dict(BENCH_PARAMS, ds=(two_pi / nx, two_pi / ny, two_pi / nz), upwind=0)
+    p.update(over)
+    return p
+
+
+def seeded_mesh(n, seed: int, amp_scalar: float = 1e-5, sigma_uu: float = 1e-3,
+                sigma_aa: float = 1e-4) -> np.ndarray:
+    """The seeded initial condition of the benchmark workloads, made by the port
+    (bytes equal to the product's acHostMeshRandomizeSeeded; the golden input
+    hashes pin both)."""
+    nx, ny, nz = (n, n, n) if np.isscalar(n) else n
+    f = np.zeros((8, nz + 6, ny + 6, nx + 6))
+    if lib("port").oracle_seeded_mesh(_ptrs(f), nx, ny, nz, seed, amp_scalar, sigma_uu,
+                                      sigma_aa) != 0:
+        raise RuntimeError("oracle seeded mesh failed")
+    return f
 
 
 def _ptrs(fields: np.ndarray):

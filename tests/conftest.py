@@ -20,8 +20,11 @@ def built():
     """Builds the product library and the oracles once per session (in-tree)."""
     from astaroth_b200 import build as b
     b.build()
-    subprocess.run(["make", "-s", "-C", str(ROOT / "oracle"),
-                    f"REF={os.environ.get('AC_REFERENCE', '/root/reference')}"], check=True)
+    # the reference model (oracle/_ref) is built where the reference tree is
+    # found: $AC_REFERENCE, else a checkout named "reference" beside the repository
+    ref = os.environ.get("AC_REFERENCE")
+    subprocess.run(["make", "-s", "-C", str(ROOT / "oracle")] + ([f"REF={ref}"] if ref else []),
+                   check=True)
     yield
 
 

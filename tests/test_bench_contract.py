@@ -39,6 +39,28 @@ def test_reference_arm_line():
     assert cb["kind"] in ("reference", "port") and cb["cores"] >= 1 and cb["sample"]
     assert cb["value"] == d["value"]
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0
+    # ms_per_step is the measured time of the timed sample, not a scaled figure
+    n = d["config"]["cpu_sample_n"]
+    assert abs(d["value"] * d["ms_per_step"] * 1e-3 - n ** 3) <= 1e-6 * n ** 3
+    assert f"{n}^3" in cb["sample"]
+
+
+def test_reference_arm_maps_no_product_library():
+    """The reference arm runs the reference's own host model with inputs made on
+    the oracle side: the product's shared library is never loaded."""
+    code = (
+        "import sys, types; sys.argv = ['bench.py']; sys.path.insert(0, '.');"
+        "import bench;"
+        "a = types.SimpleNamespace(warmup=0, steps=1, n=512, gpus=1);"
+        "import io, contextlib; buf = io.StringIO();"
+        "ctx = contextlib.redirect_stdout(buf); ctx.__enter__(); bench.run_reference(a); ctx.__exit__(None, None, None);"
+        "maps = open('/proc/self/maps').read();"
+        "print('PRODUCT' if 'libastaroth_b200' in maps else 'CLEAN');"
+        "print('ORACLE' if 'oracle/' in maps else 'NO-ORACLE')")
+    r = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True,
+                       timeout=900, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert "CLEAN" in r.stdout and "ORACLE" in r.stdout, r.stdout
 
 
 @pytest.mark.gpu

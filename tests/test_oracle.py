@@ -190,3 +190,20 @@ def test_torch_reference_matches_oracle():
         x = R.step(x, p, 2e-3)
     err = oracle.rel_linf(np.pad(x.numpy(), ((0, 0),) + ((3, 3),) * 3), a)
     assert err.max() <= 1e-14
+
+
+def test_oracle_seeded_mesh_matches_golden_and_product():
+    """The oracle-side generator (used where the product library must not be
+    loaded) gives the golden inputs' bytes and the product generator's bytes."""
+    for name, c in META["cases"].items():
+        n = c["n"] if isinstance(c["n"], int) else tuple(c["n"])
+        assert sha(oracle.seeded_mesh(n, c["seed"])) == c["input_sha256"], name
+    info = make_info((9, 7, 5), **CONFIG_PARAMS)
+    a = seeded_mesh(info, 11, amp_scalar=0.1, sigma_uu=0.05, sigma_aa=0.02)
+    b = oracle.seeded_mesh((9, 7, 5), 11, amp_scalar=0.1, sigma_uu=0.05, sigma_aa=0.02)
+    assert np.array_equal(a, b)
+    p = oracle.box_params((9, 7, 5))
+    q = info_to_dict(info)
+    for k, v in q.items():
+        assert np.allclose(p[k], v, rtol=0, atol=0), k
+

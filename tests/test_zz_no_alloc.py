@@ -63,6 +63,22 @@ def test_no_alloc_matches_existing_entry_point_twice():
                 torch.cuda.synchronize()
                 got = float(result.item())
                 assert abs(got - want) <= 8 * EPS * abs(want), (r, h, call, got, want)
+        # caller-chosen grids: one block, an odd count, and the largest the
+        # static scratch holds (more blocks than the 24 * 16 rows: the extra
+        # blocks contribute only the identity of the reduction)
+        for r, h in (("RTYPE_SUM", [0]), ("RTYPE_MAX", [1, 2, 3])):
+            want = existing(dev, r, h)
+            ptrs = (C.c_void_p * len(h))(*[fields_dev[q].data_ptr() for q in h])
+            for blocks in (1, 7, capi.AC_REDUCE_NOALLOC_MAX_BLOCKS):
+                for call in range(2):
+                    result.fill_(np.nan)
+                    rc = lib.acReduceNoAlloc(ptrs, len(h), n[0], n[1], n[2], capi.RTYPES[r],
+                                             C.c_void_p(result.data_ptr()), blocks,
+                                             C.c_void_p(stream.cuda_stream))
+                    assert rc == capi.AC_SUCCESS, (r, h, blocks, call)
+                    torch.cuda.synchronize()
+                    got = float(result.item())
+                    assert abs(got - want) <= 8 * EPS * abs(want), (r, h, blocks, got, want)
 
 
 def test_no_alloc_rejects_too_many_blocks():
@@ -77,6 +93,14 @@ def test_no_alloc_rejects_too_many_blocks():
     rc = lib.acReduceNoAlloc(ptrs, 1, 16, 16, 16, capi.RTYPES["RTYPE_SUM"],
                              C.c_void_p(result.data_ptr()), capi.AC_REDUCE_NOALLOC_MAX_BLOCKS + 1,
                              None)
+    assert rc == capi.AC_FAILURE
+    # a negative grid size is a caller error, not a request for the default
+    rc = lib.acReduceNoAlloc(ptrs, 1, 16, 16, 16, capi.RTYPES["RTYPE_SUM"],
+                             C.c_void_p(result.data_ptr()), -1, None)
+    assert rc == capi.AC_FAILURE
+    # extents whose padded size would overflow an int are refused
+    rc = lib.acReduceNoAlloc(ptrs, 1, 2147483647, 16, 16, capi.RTYPES["RTYPE_SUM"],
+                             C.c_void_p(result.data_ptr()), 0, None)
     assert rc == capi.AC_FAILURE
     # a wrong field count for the reduction type is rejected too
     rc = lib.acReduceNoAlloc(ptrs, 1, 16, 16, 16, capi.RTYPES["RTYPE_ALFVEN_MAX"],
