@@ -33,7 +33,7 @@ CU_SOURCES = ["device.cu", "device_data.cu", "device_adjoint.cu", "solve.cu", "s
               "bfield.cu"]
 C_SOURCES = ["host.c"]
 HEADERS = ["internal.h", "mhd_rhs.cuh", "mhd_rhs_adjoint.cuh", "stencil_plain.cuh", "solve_cell.cuh",
-           "halo.cuh", "tma_ring.cuh", "device_impl.h"]
+           "halo.cuh", "tma_ring.cuh", "tmem.cuh", "device_impl.h"]
 
 
 def _nvcc() -> str:

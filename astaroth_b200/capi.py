@@ -317,6 +317,7 @@ SIGNATURES = {
     "acDeviceAdjointTapeBackward": (C.c_int, [Device_p, C.c_int, C.c_int, C.c_double]),
     "acDeviceGetStreamHandle": (C.c_void_p, [Device_p, C.c_int]),
     "acDeviceGetLaunchCount": (C.c_ulonglong, [Device_p]),
+    "acDeviceDebugSkipPlaneLoad": (C.c_int, [Device_p, C.c_int]),
     "acB200Version": (C.c_char_p, []),
     "acReduceNoAlloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int, C.c_int,
                                   AcReduction, C.c_void_p, C.c_int, C.c_void_p]),

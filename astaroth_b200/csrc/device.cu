@@ -87,6 +87,7 @@ ac_make_phys(const AcMeshInfo& info, PhysConst* pc)
     pc->inv_exp_lnT0 = exp(-r[AC_lnT0]);
     pc->K            = r[AC_K_heatcond];
     pc->upwind       = info.int_params[AC_upwind] != 0;
+    pc->debug_skip_load = 0;
     pc->forcing      = 0;
     for (int a = 0; a < 3; ++a)
         pc->f_k[a] = pc->f_re[a] = pc->f_im[a] = 0.0;
@@ -97,6 +98,15 @@ ac_make_phys(const AcMeshInfo& info, PhysConst* pc)
 
 /* The forcing of a substep-2 launch (mhdsolver.ac:531-541): active when
  * AC_lforcing is set and AC_current_time > AC_switch_forcing. */
+/* AC_debug_plain_kernel: 0 = the leading-plane tiled kernel (default), 1 = the
+ * plain kernel, 2 = the per-plane tap tiled kernel */
+static int
+solve_variant_of(const AcMeshInfo& info)
+{
+    const int v = info.int_params[AC_debug_plain_kernel];
+    return v == 1 ? 0 : v == 2 ? AC_SOLVE_TILED_TAPS : AC_SOLVE_TILED_LEAD;
+}
+
 static void
 forcing_for_launch(const AcMeshInfo& info, const double dt, PhysConst* pc)
 {
@@ -240,7 +250,7 @@ acDeviceCreate(const int id, const AcMeshInfo device_config, Device* device_hand
     d->config    = info;
     d->geom      = ac_make_geom(info, precision);
     d->precision = precision;
-    d->solve_variant = info.int_params[AC_debug_plain_kernel] ? 0 : 1;
+    d->solve_variant = solve_variant_of(info);
 
 #define CREATE_CHECK(call)                                                                    \
     do {                                                                                      \
@@ -447,6 +457,18 @@ acDeviceLoadInt3Uniform(const Device d, const Stream stream, const AcInt3Param p
 }
 
 extern "C" AcResult
+acDeviceDebugSkipPlaneLoad(const Device d, const int enable)
+{
+    if (!d)
+        return AC_FAILURE;
+    if ((enable != 0) != (d->debug_skip_load != 0)) {
+        d->debug_skip_load = enable != 0;
+        invalidate_graphs(d); /* captured launches carry the switch */
+    }
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
 acDeviceLoadIntUniform(const Device d, const Stream stream, const AcIntParam param,
                        const int value)
 {
@@ -457,7 +479,7 @@ acDeviceLoadIntUniform(const Device d, const Stream stream, const AcIntParam par
     info.int_params[param] = value;
     const AcResult r       = refresh_config(d, info);
     if (r == AC_SUCCESS)
-        d->solve_variant = d->config.int_params[AC_debug_plain_kernel] ? 0 : 1;
+        d->solve_variant = solve_variant_of(d->config);
     return r;
 }
 
@@ -684,6 +706,7 @@ launch_substep(Device d, cudaStream_t st, const int step, const double dt,
     PhysConst pc;
     ac_make_stencil(d->config, &sc);
     ac_make_phys(d->config, &pc);
+    pc.debug_skip_load = d->debug_skip_load;
     if (step == 2)
         forcing_for_launch(d->config, dt, &pc);
     const RkCoef rk = ac_rk_coef(step, dt);
@@ -703,7 +726,7 @@ launch_substep(Device d, cudaStream_t st, const int step, const double dt,
             return e;
     }
     const int blk   = in_block_index(d);
-    const bool tiled = d->solve_variant == 1 && d->tmap_ok && blk >= 0;
+    const bool tiled = d->solve_variant != 0 && d->tmap_ok && blk >= 0;
     /* substep 2 also produces the CFL maxima of its input state, as the
      * reference's calc_timestep inside the third substep (mhdsolver.ac:611) */
     unsigned long long* cfl = nullptr;
@@ -717,13 +740,13 @@ launch_substep(Device d, cudaStream_t st, const int step, const double dt,
     if (d->precision == 0) {
         const Fields64 f = fields64(d);
         e = tiled ? ac_launch_solve_tiled64(d->geom, &d->tmap[blk], f, sc, pc, rk, d->err_flag,
-                                            cfl, st, launches)
+                                            cfl, st, launches, d->solve_variant)
                   : ac_launch_solve_plain64(d->geom, f, sc, pc, rk, cfl, st, launches);
     }
     else {
         const Fields32 f = fields32(d);
         e = tiled ? ac_launch_solve_tiled32(d->geom, &d->tmap[blk], f, sc, pc, rk, d->err_flag,
-                                            cfl, st, launches)
+                                            cfl, st, launches, d->solve_variant)
                   : ac_launch_solve_plain32(d->geom, f, sc, pc, rk, cfl, st, launches);
     }
     if (e != cudaSuccess || !pc.forcing)

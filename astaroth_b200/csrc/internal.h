@@ -56,6 +56,7 @@ struct PhysConst {
     double inv_exp_lnT0;  /* exp(-lnT0) */
     double K;             /* K_heatcond */
     int upwind;           /* AC_upwind: the LUPWD terms (selects the kernel variant) */
+    int debug_skip_load;  /* acDeviceDebugSkipPlaneLoad: the fault-path test of the tiled kernels */
     /* helical forcing of this launch (substep 2 only; forcing = 0 otherwise):
      * u += scale (re cos(a + phase) - im sin(a + phase)), a = sum_d f_k[d] idx_d
      * with idx the interior cell index (mhdsolver.ac:286-331) */
@@ -165,7 +166,8 @@ struct device_s {
     ReduceScratch red;
     double* host_result; /* pinned */
     StepGraph graphs[NUM_STREAMS][2];
-    int solve_variant;   /* 0 = plain, 1 = tiled */
+    int solve_variant;   /* 0 = plain, else the tiled kernel AC_SOLVE_TILED_* */
+    int debug_skip_load; /* acDeviceDebugSkipPlaneLoad */
     /* adjoint buffers, allocated by the first acDeviceLoadAdjoint */
     double* adj_lf;      /* 8 fields */
     double* adj_lw;      /* 8 fields */
@@ -251,17 +253,22 @@ cudaError_t ac_launch_reduce(const Geom& g, const void* const* fields, const flo
 
 int ac_reduce_blocks(const Geom& g);
 
+/* Tiled substep kernels (solve_tiled.cu): the leading-plane kernel (in-plane
+ * derivatives of plane z+3 kept in tensor memory until plane z is solved;
+ * the default) and the per-plane tap kernel.  Meshes with the upwinding
+ * terms always take the per-plane tap kernel. */
+enum { AC_SOLVE_TILED_LEAD = 1, AC_SOLVE_TILED_TAPS = 2 };
 bool ac_tiled_supported(const Geom& g, const int precision);
 bool ac_make_tensor_map(void* map_out, void* base, const Geom& g, const int precision);
 cudaError_t ac_solve_tiled_init(const int precision);
 cudaError_t ac_launch_solve_tiled64(const Geom& g, const void* tmap_in, const Fields64& f,
                                     const StencilCoef& sc, const PhysConst& pc, const RkCoef& rk,
                                     int* err, unsigned long long* cfl, cudaStream_t stream,
-                                    unsigned long long* launches);
+                                    unsigned long long* launches, const int kernel);
 cudaError_t ac_launch_solve_tiled32(const Geom& g, const void* tmap_in, const Fields32& f,
                                     const StencilCoef& sc, const PhysConst& pc, const RkCoef& rk,
                                     int* err, unsigned long long* cfl, cudaStream_t stream,
-                                    unsigned long long* launches);
+                                    unsigned long long* launches, const int kernel);
 
 /* Helical forcing added to the three velocity arrays u (and their
  * compensation arrays lo in FP32) after substep 2 (forcing.cu). */

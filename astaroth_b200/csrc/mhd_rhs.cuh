@@ -150,6 +150,33 @@ hydro_prepare(const ScalD<T>& L, const T s_value, const VecD<T>& U, const PhysT<
     x.a[H2M_LAPL] = L.lap;
 }
 
+/* hydro_prepare with the two exponentials (H2M_E and H2M_INV_RHO, the same
+ * expressions) formed beforehand */
+template <typename T>
+__device__ __forceinline__ void
+hydro_prepare_exp(const ScalD<T>& L, const VecD<T>& U, const T e, const T inv_rho,
+                  HydroToMag<T>& x, Strain<T>& S)
+{
+    const T third     = (T)(1.0 / 3.0);
+    x.a[H2M_DIVU]     = U.g[0][0] + U.g[1][1] + U.g[2][2];
+    S.S00 = (T)(2.0 / 3.0) * U.g[0][0] - third * (U.g[1][1] + U.g[2][2]);
+    S.S11 = (T)(2.0 / 3.0) * U.g[1][1] - third * (U.g[0][0] + U.g[2][2]);
+    S.S22 = (T)(2.0 / 3.0) * U.g[2][2] - third * (U.g[0][0] + U.g[1][1]);
+    S.S01 = (T)0.5 * (U.g[0][1] + U.g[1][0]);
+    S.S02 = (T)0.5 * (U.g[0][2] + U.g[2][0]);
+    S.S12 = (T)0.5 * (U.g[1][2] + U.g[2][1]);
+    x.a[H2M_SS] = S.S00 * S.S00 + S.S11 * S.S11 + S.S22 * S.S22 +
+                  (T)2 * (S.S01 * S.S01 + S.S02 * S.S02 + S.S12 * S.S12);
+    x.a[H2M_E]       = e;
+    x.a[H2M_INV_RHO] = inv_rho;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        x.a[H2M_U + a]  = U.v[a];
+        x.a[H2M_GL + a] = L.g[a];
+    }
+    x.a[H2M_LAPL] = L.lap;
+}
+
 template <typename T>
 __device__ __forceinline__ void
 mag_prepare(const ScalD<T>& Sg, const VecD<T>& A, const PhysT<T>& p, MagToHydro<T>& m)

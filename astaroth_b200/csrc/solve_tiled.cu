@@ -35,6 +35,7 @@
 #include "internal.h"
 #include "mhd_rhs.cuh"
 #include "tma_ring.cuh"
+#include "tmem.cuh"
 
 namespace {
 
@@ -70,6 +71,18 @@ struct Layout {
     static constexpr size_t SMEM_BYTES   = (size_t)RING * SLOT_BYTES + (size_t)XCHG * sizeof(T) +
                                          RING * sizeof(uint64_t);
 };
+
+/* Number of plane loads issued into ring slot sl for the planes pfirst .. plast
+ * (plane p goes to slot (p - pfirst) mod RING), without plast when skipped. */
+__device__ __forceinline__ int
+loads_into(const int sl, const int pfirst, const int plast, const bool skip_last)
+{
+    const int np = plast - pfirst + 1;
+    int n        = sl < np ? (np - 1 - sl) / RING + 1 : 0;
+    if (skip_last && ((plast - pfirst) & (RING - 1)) == sl)
+        --n;
+    return n;
+}
 
 /* Taps of field q at offset (dx, dy, dz) from this thread's cell. */
 template <typename T>
@@ -242,9 +255,14 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
         fence_barrier_init();
     }
     __syncthreads();
+    /* the fault-path test switch skips the load of plane plast */
+    const bool skip_last  = pc.debug_skip_load != 0;
+    const long long wlim  = skip_last ? kDebugWaitLimit : kWaitLimit;
     if (tid == 0) {
         const int pend = min(plast, pfirst + RING - 1);
         for (int p = pfirst; p <= pend; ++p) {
+            if (skip_last && p == plast)
+                continue;
             const int s = (p - pfirst) & (RING - 1);
             mbar_arrive_expect_tx(&bars[s], L::SLOT_BYTES);
             tma_load_plane(smem + (size_t)s * L::SLOT, &tmap, &bars[s], x0, y0, p + NGHOST);
@@ -297,7 +315,7 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
             const int s = (q - pfirst) & (RING - 1);
             /* after one failed wait the kernel stops waiting and only runs out */
             if (ok)
-                ok = mbar_wait_bounded(&bars[s], (unsigned)(((q - pfirst) / RING) & 1));
+                ok = mbar_wait_bounded(&bars[s], (unsigned)(((q - pfirst) / RING) & 1), wlim);
         }
         waited = z + NGHOST;
 
@@ -428,7 +446,7 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
         }
         __syncthreads(); /* every thread is done with plane z - 3 and the exchange */
         const int next = z - NGHOST + RING;
-        if (tid == 0 && next <= plast) {
+        if (tid == 0 && next <= plast && !(skip_last && next == plast)) {
             const int s = (next - pfirst) & (RING - 1);
             mbar_arrive_expect_tx(&bars[s], L::SLOT_BYTES);
             tma_load_plane(smem + (size_t)s * L::SLOT, &tmap, &bars[s], x0, y0, next + NGHOST);
@@ -438,6 +456,592 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
         cfl_commit(cm, xh, cfl); /* the exchange area is free after the last barrier */
     if (!ok)
         atomicExch(err, 1);
+    if (tid == 0)
+        drain_ring(bars, RING, [&](const int sl) { return loads_into(sl, pfirst, plast, skip_last); });
+}
+
+/* ---------------------------------------------------------------------------
+ * The leading-plane substep kernel: the production path for meshes without
+ * the upwinding terms.
+ *
+ * Same tiles, plane ring, warp groups and RHS as solve_tiled_kernel, with the
+ * stencils reorganised so that each in-plane tap is read from shared memory
+ * once and serves every derivative that needs it:
+ *
+ * * When plane L arrives, each thread forms the x and y differences
+ *   D^k f = f(+k) - f(-k) and sums S^k = f(+k) + f(-k) (k = 1..3) of its
+ *   group's fields at its cell, and from them the in-plane first and second
+ *   derivatives and the diagonal xy mixed derivatives of plane L.  These 17
+ *   values per group (its record) go to tensor memory (TMEM), a 4-plane delay
+ *   line in the thread's own lane, and come back when plane L is solved three
+ *   planes later (the z stencils need planes up to z + 3 first).
+ * * The xz and yz mixed derivatives use the separable form of the diagonal
+ *   stencil (derivs.h:591-690):  D_az f(z) = sum_k e_k [D_a^k f(z+k) - D_a^k f(z-k)]
+ *   with a = x or y.  The differences D_a^k at plane L are the ones just
+ *   formed, so each mixed derivative costs no further shared-memory reads:
+ *   plane L adds +e_k D^k to the sum of plane L-k and -e_k D^k to that of
+ *   plane L+k, in seven running sums per mixed term held in registers.  Only
+ *   the combinations grad(div) needs are formed: D_xz uz, D_yz uz and
+ *   D_xz ux + D_yz uy (and the same for aa).
+ * * The z first and second derivatives of the vector components still read the
+ *   plane ring at plane z (their own column); the scalar field keeps its z
+ *   line in registers.
+ *
+ * Per cell and substep this reads ~200 values from shared memory instead of
+ * ~320.  The arithmetic per cell is the same up to association (the mixed
+ * derivatives are summed in a different order), so results agree with the
+ * other kernels to rounding, not bit for bit.
+ * ------------------------------------------------------------------------- */
+template <typename T>
+struct LeadTm;
+template <>
+struct LeadTm<double> {
+    static constexpr uint32_t NCOLS = 512; /* 1 block per SM */
+    static constexpr uint32_t GROUP = 256; /* columns per warp group */
+    static constexpr uint32_t SLOT  = 64;  /* columns per plane record */
+};
+template <>
+struct LeadTm<float> {
+    static constexpr uint32_t NCOLS = 256; /* 2 blocks per SM */
+    static constexpr uint32_t GROUP = 128;
+    static constexpr uint32_t SLOT  = 32;
+};
+
+/* record of one plane and warp group (index: value) */
+constexpr int NREC      = 19;
+constexpr int REC_SD1X  = 0;  /* scalar d/dx */
+constexpr int REC_SD1Y  = 1;  /* scalar d/dy */
+constexpr int REC_SLAP  = 2;  /* scalar second-derivative side sums, x + y */
+constexpr int REC_V     = 3;  /* + 4c + {0: d/dx, 1: d/dy, 2: x sides, 3: y sides} of component c */
+constexpr int REC_DXY0  = 15; /* D_xy of component 0 (enters grad div, y) */
+constexpr int REC_E     = 16; /* group 0 only: exp(gamma s/cp + (gamma-1)(lnrho - lnrho0)) */
+constexpr int REC_IRHO  = 17; /* group 0 only: exp(-lnrho) */
+constexpr int REC_DXY1  = 18; /* D_xy of component 1 (enters grad div, x) */
+
+template <typename T>
+constexpr size_t lead_smem_bytes()
+{
+    return Layout<T>::SMEM_BYTES + 16; /* + the TMEM base address */
+}
+
+/* Column offsets of a record's three parts: A = entries 0..15, B = 16..17 (the
+ * two exponentials), C = entry 18; as 32-bit words (two per double). */
+template <typename T>
+struct RecCols {
+    static constexpr int WE = (int)sizeof(T) / 4; /* words per entry */
+    static constexpr int B  = 16 * WE;
+    static constexpr int C  = 18 * WE;
+};
+
+template <typename T, bool WITH_B>
+__device__ __forceinline__ void
+rec_store(const uint32_t a, const tmem::Words<T, NREC>& r)
+{
+    typedef RecCols<T> RC;
+    if constexpr (sizeof(T) == 8) {
+        tmem::st32(a, r.w);
+        if constexpr (WITH_B)
+            tmem::st4(a + RC::B, r.w + RC::B);
+        tmem::st2(a + RC::C, r.w + RC::C);
+    }
+    else {
+        tmem::st16(a, r.w);
+        if constexpr (WITH_B)
+            tmem::st2(a + RC::B, r.w + RC::B);
+        tmem::st1(a + RC::C, r.w[RC::C]);
+    }
+}
+
+template <typename T, bool WITH_B>
+__device__ __forceinline__ void
+rec_load(const uint32_t a, tmem::Words<T, NREC>& r)
+{
+    typedef RecCols<T> RC;
+    if constexpr (sizeof(T) == 8) {
+        tmem::ld32(a, r.w);
+        if constexpr (WITH_B)
+            tmem::ld4(a + RC::B, r.w + RC::B);
+        tmem::ld2(a + RC::C, r.w + RC::C);
+    }
+    else {
+        tmem::ld16(a, r.w);
+        if constexpr (WITH_B)
+            tmem::ld2(a + RC::B, r.w + RC::B);
+        tmem::ld1(a + RC::C, r.w + RC::C);
+    }
+}
+
+/* part B alone (the exponentials of another group's record) */
+template <typename T>
+__device__ __forceinline__ void
+rec_load_b(const uint32_t a, tmem::Words<T, NREC>& r)
+{
+    typedef RecCols<T> RC;
+    if constexpr (sizeof(T) == 8)
+        tmem::ld4(a + RC::B, r.w + RC::B);
+    else
+        tmem::ld2(a + RC::B, r.w + RC::B);
+}
+
+/* differences and sums of one field along x (or y) at this cell of a plane:
+ * p points at the field's value there; step is 1 (x) or the row pitch (y) */
+template <typename T>
+__device__ __forceinline__ void
+diffs(const T* p, const int step, T d[3])
+{
+#pragma unroll
+    for (int k = 1; k <= 3; ++k)
+        d[k - 1] = p[k * step] - p[-k * step];
+}
+
+template <typename T>
+__device__ __forceinline__ void
+diffs_sums(const T* p, const int step, T d[3], T s[3])
+{
+#pragma unroll
+    for (int k = 1; k <= 3; ++k) {
+        const T a = p[k * step], b = p[-k * step];
+        d[k - 1]  = a - b;
+        s[k - 1]  = a + b;
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T
+d1_from(const T d[3], const T* c)
+{
+    T r = c[0] * d[0];
+    r   = fma(c[1], d[1], r);
+    r   = fma(c[2], d[2], r);
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ T
+d2s_from(const T s[3], const T* c)
+{
+    T r = c[1] * s[0];
+    r   = fma(c[2], s[1], r);
+    r   = fma(c[3], s[2], r);
+    return r;
+}
+
+/* diagonal xy mixed derivative at this cell of a plane (12 taps) */
+template <typename T>
+__device__ __forceinline__ T
+dxy_at(const T* p, const T* e)
+{
+    constexpr int H = Layout<T>::HXP;
+    T r             = 0;
+#pragma unroll
+    for (int k = 1; k <= 3; ++k) {
+        const T s = (p[k + k * H] + p[-k - k * H]) - (p[k - k * H] + p[-k + k * H]);
+        r         = k == 1 ? e[0] * s : fma(e[k - 1], s, r);
+    }
+    return r;
+}
+
+template <bool I, bool S>
+struct LeadPhase {
+    static constexpr bool interior = I; /* the plane arriving is interior: its record is kept */
+    static constexpr bool solve    = S; /* plane lp - 3 is solved in this step */
+};
+
+/* The whole chunk for the threads of one warp group (GROUP 0: lnrho and uu,
+ * GROUP 1: aa and entropy).  Both groups take the same barriers in the same
+ * order. */
+template <typename T, bool COMP, int GROUP>
+__device__ __forceinline__ void
+lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const StencilT<T>& sc,
+           const PhysT<T>& p, const RkCoef& rk, int* err, unsigned long long* cfl, T* smem, T* xh,
+           T* xm, uint64_t* bars, const uint32_t tcol, const int zchunk, const bool skip_last)
+{
+    const long long wlim = skip_last ? kDebugWaitLimit : kWaitLimit;
+    typedef Layout<T> L;
+    typedef LeadTm<T> TM;
+    constexpr int QS = GROUP == 0 ? VTXBUF_LNRHO : VTXBUF_ENTROPY;
+    constexpr int Q0 = GROUP == 0 ? VTXBUF_UUX : VTXBUF_AX;
+    constexpr int NW = tmem::Words<T, NREC>::W;
+    const int lx     = threadIdx.x;
+    const int ly     = threadIdx.y & (TY - 1);
+    const int tid    = threadIdx.y * TX + lx;
+    const int cell   = ly * TX + lx;
+    const int x0     = blockIdx.x * TX;
+    const int y0     = blockIdx.y * TY;
+    const int z0     = blockIdx.z * zchunk;
+    const int z1     = min(z0 + zchunk, g.nz);
+    const int pfirst = z0 - NGHOST;
+    const int plast  = z1 - 1 + NGHOST;
+    const int x = x0 + lx, y = y0 + ly;
+    const bool active   = x < g.nx && y < g.ny;
+    const bool use_prev = rk.step > 0;
+    const int cell_off  = (ly + NGHOST) * L::HXP + (lx + NGHOST);
+    T* outp[4];
+    T* outl[4];
+    const T* inl[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        outp[k] = f.out[4 * GROUP + k];
+        outl[k] = f.out_lo[4 * GROUP + k];
+        inl[k]  = f.in_lo[4 * GROUP + k];
+    }
+    bool ok    = true;
+    int waited = pfirst - 1;
+    T cm[3]    = {0, 0, 0};
+    T zq[7]    = {0, 0, 0, 0, 0, 0, 0}; /* the scalar field at this cell, planes z-3 .. z+3 */
+    /* running sums of the z-coupled mixed terms of grad(div) of this group's
+     * vector v for planes lp-3 .. lp+3: [0] D_xz v_z, [1] D_yz v_z,
+     * [2] D_xz v_x + D_yz v_y */
+    T acc[3][7];
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int j = 0; j < 7; ++j)
+            acc[a][j] = 0;
+
+    auto step = [&](auto ph, const int lp) {
+        constexpr bool INTERIOR = decltype(ph)::interior;
+        constexpr bool SOLVE    = decltype(ph)::solve;
+        const int z             = lp - NGHOST; /* the plane solved in this step */
+        const long long idx     = geom_idx(g, x + NGHOST, y + NGHOST, z + NGHOST);
+        T prev[4] = {0, 0, 0, 0}, prevl[4] = {0, 0, 0, 0}, lo[4] = {0, 0, 0, 0};
+        if constexpr (SOLVE) {
+            if (active) {
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if (use_prev)
+                        prev[k] = outp[k][idx];
+                    if (COMP) {
+                        lo[k] = inl[k][idx];
+                        if (use_prev)
+                            prevl[k] = outl[k][idx];
+                    }
+                }
+            }
+        }
+        for (int q = waited + 1; q <= lp; ++q) {
+            const int s = (q - pfirst) & (RING - 1);
+            if (ok)
+                ok = mbar_wait_bounded(&bars[s], (unsigned)(((q - pfirst) / RING) & 1), wlim);
+        }
+        waited = lp;
+        __syncwarp(); /* tensor-memory accesses below are warp-collective */
+
+        /* record of plane z, stored three steps ago */
+        tmem::Words<T, NREC> rz;
+        if constexpr (SOLVE) {
+            rec_load<T, GROUP == 0>(tcol + (uint32_t)(z & 3) * TM::SLOT, rz);
+            if constexpr (GROUP == 1) /* the exponentials from group 0's record of plane z */
+                rec_load_b<T>(tcol - TM::GROUP + (uint32_t)(z & 3) * TM::SLOT, rz);
+        }
+
+        /* ---- plane lp: in-plane differences, record, running mixed sums ---- */
+        const T* pl = smem + (size_t)((lp - pfirst) & (RING - 1)) * L::SLOT + cell_off;
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+            zq[k] = zq[k + 1];
+        zq[6] = pl[QS * L::PLANE];
+        T dvx[3], dvy[3], dzx[3], dzy[3]; /* D_x^k v_x, D_y^k v_y, D_x^k v_z, D_y^k v_z */
+        if constexpr (INTERIOR) {
+            tmem::Words<T, NREC> r;
+            {
+                const T* ps = pl + QS * L::PLANE;
+                T d[3], s[3], e[3], t[3];
+                diffs_sums(ps, 1, d, s);
+                diffs_sums(ps, L::HXP, e, t);
+                r.set(REC_SD1X, d1_from(d, sc.d1[0]));
+                r.set(REC_SD1Y, d1_from(e, sc.d1[1]));
+                r.set(REC_SLAP, d2s_from(s, sc.d2[0]) + d2s_from(t, sc.d2[1]));
+            }
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const T* pv = pl + (Q0 + c) * L::PLANE;
+                T d[3], s[3], e[3], t[3];
+                diffs_sums(pv, 1, d, s);
+                diffs_sums(pv, L::HXP, e, t);
+                r.set(REC_V + 4 * c + 0, d1_from(d, sc.d1[0]));
+                r.set(REC_V + 4 * c + 1, d1_from(e, sc.d1[1]));
+                r.set(REC_V + 4 * c + 2, d2s_from(s, sc.d2[0]));
+                r.set(REC_V + 4 * c + 3, d2s_from(t, sc.d2[1]));
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    if (c == 0)
+                        dvx[k] = d[k];
+                    if (c == 1)
+                        dvy[k] = e[k];
+                    if (c == 2) {
+                        dzx[k] = d[k];
+                        dzy[k] = e[k];
+                    }
+                }
+            }
+            r.set(REC_DXY0, dxy_at(pl + Q0 * L::PLANE, sc.mix[0]));
+            r.set(REC_DXY1, dxy_at(pl + (Q0 + 1) * L::PLANE, sc.mix[0]));
+            if constexpr (GROUP == 0) {
+                /* the two exponentials of the RHS (the expressions of
+                 * hydro_prepare), for both groups, off the solve's critical path */
+                const T lv  = zq[6];
+                const T sv  = pl[VTXBUF_ENTROPY * L::PLANE];
+                const T arg = p.gamma_inv_cp * sv + p.gamma_m1 * (lv - p.lnrho0);
+                r.set(REC_E, ac_exp(arg));
+                r.set(REC_IRHO, ac_exp(-lv));
+            }
+            rec_store<T, GROUP == 0>(tcol + (uint32_t)(lp & 3) * TM::SLOT, r);
+        }
+        else {
+            /* halo planes only feed the mixed sums */
+            diffs(pl + Q0 * L::PLANE, 1, dvx);
+            diffs(pl + (Q0 + 1) * L::PLANE, L::HXP, dvy);
+            diffs(pl + (Q0 + 2) * L::PLANE, 1, dzx);
+            diffs(pl + (Q0 + 2) * L::PLANE, L::HXP, dzy);
+        }
+#pragma unroll
+        for (int k = 1; k <= 3; ++k) {
+            const T exz = sc.mix[1][k - 1], eyz = sc.mix[2][k - 1];
+            const T a0  = exz * dzx[k - 1];
+            const T a1  = eyz * dzy[k - 1];
+            const T a2  = fma(exz, dvx[k - 1], eyz * dvy[k - 1]);
+            acc[0][3 - k] += a0;
+            acc[0][3 + k] -= a0;
+            acc[1][3 - k] += a1;
+            acc[1][3 + k] -= a1;
+            acc[2][3 - k] += a2;
+            acc[2][3 + k] -= a2;
+        }
+
+        /* ---- plane z = lp - 3: the RHS and the RK update ---- */
+        if constexpr (SOLVE) {
+            Taps<T> t;
+            t.s = smem;
+#pragma unroll
+            for (int k = 0; k < 7; ++k)
+                t.off[k] = ((z - NGHOST + k - pfirst) & (RING - 1)) * L::SLOT + cell_off;
+            ScalD<T> sd;
+            VecD<T> vd;
+            T s2z[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const int q = Q0 + c;
+                vd.v[c]     = t(q, 0, 0, 0);
+                vd.g[c][2]  = d1<2>(t, q, sc.d1[2]);
+                s2z[c]      = d2_sides<2>(t, q, sc.d2[2]);
+            }
+            T sz1, sz2;
+            {
+                const T* c = sc.d1[2];
+                T a        = c[0] * (zq[4] - zq[2]);
+                a          = fma(c[1], zq[5] - zq[1], a);
+                sz1        = fma(c[2], zq[6] - zq[0], a);
+                const T* d = sc.d2[2];
+                T b        = d[1] * (zq[4] + zq[2]);
+                b          = fma(d[2], zq[5] + zq[1], b);
+                sz2        = fma(d[3], zq[6] + zq[0], b);
+            }
+            tmem::wait_ld_tied<NW>(rz.w);
+            const T csum = sc.d2[0][0] + sc.d2[1][0] + sc.d2[2][0];
+            sd.v         = zq[3];
+            sd.g[0]      = rz.get(REC_SD1X);
+            sd.g[1]      = rz.get(REC_SD1Y);
+            sd.g[2]      = sz1;
+            sd.lap       = csum * sd.v + rz.get(REC_SLAP) + sz2;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                vd.g[c][0] = rz.get(REC_V + 4 * c + 0);
+                vd.g[c][1] = rz.get(REC_V + 4 * c + 1);
+                vd.lap[c]  = csum * vd.v[c] + rz.get(REC_V + 4 * c + 2) +
+                            rz.get(REC_V + 4 * c + 3) + s2z[c];
+            }
+            vd.gd[0] = sc.d2[0][0] * vd.v[0] + rz.get(REC_V + 2) + rz.get(REC_DXY1) + acc[0][0];
+            vd.gd[1] = rz.get(REC_DXY0) + sc.d2[1][0] * vd.v[1] + rz.get(REC_V + 4 + 3) + acc[1][0];
+            vd.gd[2] = acc[2][0] + sc.d2[2][0] * vd.v[2] + s2z[2];
+
+            HydroToMag<T> hx;
+            MagToHydro<T> mx;
+            [[maybe_unused]] Strain<T> st;
+            /* group 0 sends grad lnrho, lap lnrho, S:S and div u; group 1 takes u
+             * from the ring and the exponentials from group 0's record */
+            constexpr int k0 = H2M_GL, k1 = H2M_DIVU + 1;
+            if constexpr (GROUP == 0) {
+                hydro_prepare_exp(sd, vd, rz.get(REC_E), rz.get(REC_IRHO), hx, st);
+#pragma unroll
+                for (int k = k0; k < k1; ++k)
+                    xh[k * NCELL + cell] = hx.a[k];
+            }
+            else {
+                mag_prepare(sd, vd, p, mx);
+                hx.a[H2M_E]       = rz.get(REC_E);
+                hx.a[H2M_INV_RHO] = rz.get(REC_IRHO);
+                hx.a[H2M_U + 0]   = t(VTXBUF_UUX, 0, 0, 0);
+                hx.a[H2M_U + 1]   = t(VTXBUF_UUY, 0, 0, 0);
+                hx.a[H2M_U + 2]   = t(VTXBUF_UUZ, 0, 0, 0);
+#pragma unroll
+                for (int k = 0; k < AC_M2H_COUNT; ++k)
+                    xm[k * NCELL + cell] = mx.a[k];
+            }
+            __syncthreads(); /* exchange records written */
+            if (active) {
+                T rr[4], val[4];
+                if constexpr (GROUP == 0) {
+#pragma unroll
+                    for (int k = 0; k < AC_M2H_COUNT; ++k)
+                        mx.a[k] = xm[k * NCELL + cell];
+                    hydro_rates(sd, vd, st, hx, mx, p, rr);
+                    val[0] = sd.v;
+                    val[1] = vd.v[0];
+                    val[2] = vd.v[1];
+                    val[3] = vd.v[2];
+                }
+                else {
+#pragma unroll
+                    for (int k = k0; k < k1; ++k)
+                        hx.a[k] = xh[k * NCELL + cell];
+                    mag_rates(sd, vd, mx, hx, p, rr);
+                    if (cfl) {
+                        const T* u = &hx.a[H2M_U];
+                        const T* B = &mx.a[M2H_B];
+                        cfl_accumulate(u[0] * u[0] + u[1] * u[1] + u[2] * u[2],
+                                       B[0] * B[0] + B[1] * B[1] + B[2] * B[2],
+                                       hx.a[H2M_INV_RHO], p.cs2_sound, cm);
+                    }
+                    val[0] = vd.v[0];
+                    val[1] = vd.v[1];
+                    val[2] = vd.v[2];
+                    val[3] = sd.v;
+                }
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    if constexpr (COMP) {
+                        const RkT32 c = {(float)rk.dt, (float)rk.beta, (float)rk.ab};
+                        float oh, ol;
+                        rk_update_comp(val[k], lo[k], prev[k], prevl[k], rr[k], c, use_prev, oh,
+                                       ol);
+                        outp[k][idx] = oh;
+                        outl[k][idx] = ol;
+                    }
+                    else {
+                        const RkT64 c = {rk.dt, rk.beta, rk.ab};
+                        double o;
+                        rk_update(val[k], prev[k], rr[k], c, use_prev, o);
+                        outp[k][idx] = o;
+                    }
+                }
+            }
+        }
+        /* the running sums move on by one plane (the first is complete and used) */
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+#pragma unroll
+            for (int j = 0; j < 6; ++j)
+                acc[a][j] = acc[a][j + 1];
+            acc[a][6] = 0;
+        }
+        /* every thread is done with plane lp - 6 and the exchange; the records
+         * stored in this step are visible to the other group after the barrier */
+        tmem::wait_st();
+        tmem::fence_before_sync();
+        __syncthreads();
+        tmem::fence_after_sync();
+        if constexpr (SOLVE) {
+            const int next = lp + 2; /* = lp - 6 + RING, in the slot of plane lp - 6 */
+            if (tid == 0 && next <= plast && !(skip_last && next == plast)) {
+                const int s = (next - pfirst) & (RING - 1);
+                mbar_arrive_expect_tx(&bars[s], L::SLOT_BYTES);
+                tma_load_plane(smem + (size_t)s * L::SLOT, tmap, &bars[s], x0, y0, next + NGHOST);
+            }
+        }
+    };
+
+    /* planes lp = pfirst .. plast in four phases (interior: lp in [z0, z1);
+     * solve: lp >= z0 + 3) */
+    int lp = pfirst;
+    for (; lp < z0; ++lp)
+        step(LeadPhase<false, false>{}, lp);
+    for (; lp < min(z1, z0 + NGHOST); ++lp)
+        step(LeadPhase<true, false>{}, lp);
+    for (; lp < z1; ++lp)
+        step(LeadPhase<true, true>{}, lp);
+    for (; lp < z0 + NGHOST; ++lp) /* chunks shorter than three planes */
+        step(LeadPhase<false, false>{}, lp);
+    for (; lp <= plast; ++lp)
+        step(LeadPhase<false, true>{}, lp);
+
+    if (cfl)
+        cfl_commit(cm, xh, cfl);
+    if (!ok)
+        atomicExch(err, 1);
+}
+
+template <typename T, bool COMP>
+__global__ void __launch_bounds__(2 * TX * TY, Tile<T>::MINB)
+solve_lead_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const FieldsT<T> f,
+                  const StencilT<T> sc, const PhysConst pc, const RkCoef rk, int* err,
+                  unsigned long long* cfl, const int zchunk)
+{
+    typedef Layout<T> L;
+    typedef LeadTm<T> TM;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    T* smem         = reinterpret_cast<T*>(smem_raw);
+    T* xh           = smem + (size_t)RING * L::SLOT;
+    T* xm           = xh + (size_t)AC_H2M_COUNT * NCELL;
+    uint64_t* bars  = reinterpret_cast<uint64_t*>(smem_raw + (size_t)RING * L::SLOT_BYTES +
+                                                 (size_t)XCHG * sizeof(T));
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + RING);
+    const int warp  = threadIdx.y; /* blockDim.x == 32 */
+    const int group = threadIdx.y / TY;
+    const int tid   = threadIdx.y * TX + threadIdx.x;
+    const int z0    = blockIdx.z * zchunk;
+    const int z1    = min(z0 + zchunk, g.nz);
+    const int pfirst = z0 - NGHOST;
+    const int plast  = z1 - 1 + NGHOST;
+
+    if (tid == 0) {
+        for (int s = 0; s < RING; ++s)
+            mbar_init(&bars[s], 1);
+        fence_barrier_init();
+    }
+    __syncwarp(); /* warp 0 reconverges after thread 0's barrier set-up */
+    if (warp == 0)
+        tmem::alloc(tslot, TM::NCOLS);
+    tmem::fence_before_sync();
+    __syncthreads();
+    tmem::fence_after_sync();
+    const uint32_t tbase = *tslot;
+    /* this thread's lane (its cell; both groups share it) and its group's columns */
+    const uint32_t tcol = tmem::lane_base(tbase, warp) + (uint32_t)group * TM::GROUP;
+    /* the fault-path test switch skips the load of plane plast */
+    const bool skip_last = pc.debug_skip_load != 0;
+    if (tid == 0) {
+        const int pend = min(plast, pfirst + RING - 1);
+        for (int q = pfirst; q <= pend; ++q) {
+            if (skip_last && q == plast)
+                continue;
+            const int s = (q - pfirst) & (RING - 1);
+            mbar_arrive_expect_tx(&bars[s], L::SLOT_BYTES);
+            tma_load_plane(smem + (size_t)s * L::SLOT, &tmap, &bars[s], blockIdx.x * TX,
+                           blockIdx.y * TY, q + NGHOST);
+        }
+    }
+    const PhysT<T> p        = phys_cast<T>(pc);
+    const StencilT<T> scv   = sc;
+    if (group == 0)
+        lead_group<T, COMP, 0>(&tmap, g, f, scv, p, rk, err, cfl, smem, xh, xm, bars, tcol,
+                               zchunk, skip_last);
+    else
+        lead_group<T, COMP, 1>(&tmap, g, f, scv, p, rk, err, cfl, smem, xh, xm, bars, tcol,
+                               zchunk, skip_last);
+    /* no copy into this block's shared memory is left in flight */
+    if (tid == 0)
+        drain_ring(bars, RING, [&](const int sl) { return loads_into(sl, pfirst, plast, skip_last); });
+
+    /* every thread's tensor-memory accesses are complete before the columns are freed */
+    __syncwarp();
+    tmem::wait_st();
+    tmem::fence_before_sync();
+    __syncthreads();
+    tmem::fence_after_sync();
+    __syncwarp();
+    if (warp == 0)
+        tmem::dealloc(tbase, TM::NCOLS);
 }
 
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
@@ -477,7 +1081,7 @@ template <typename T, bool COMP>
 cudaError_t
 launch_tiled(const Geom& g, const void* tmap_in, const FieldsT<T>& f, const StencilCoef& sc,
              const PhysConst& pc, const RkCoef& rk, int* err, unsigned long long* cfl,
-             cudaStream_t stream, unsigned long long* launches)
+             cudaStream_t stream, unsigned long long* launches, const int kernel)
 {
     const dim3 tpb(TX, 2 * TY, 1);
     const int zc = zchunk_for(g);
@@ -485,12 +1089,22 @@ launch_tiled(const Geom& g, const void* tmap_in, const FieldsT<T>& f, const Sten
     if (pc.upwind)
         solve_tiled_kernel<T, COMP, true><<<bpg, tpb, Layout<T>::SMEM_BYTES, stream>>>(
             *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err, cfl, zc);
+    else if (kernel == AC_SOLVE_TILED_LEAD)
+        solve_lead_kernel<T, COMP><<<bpg, tpb, lead_smem_bytes<T>(), stream>>>(
+            *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err, cfl, zc);
     else
         solve_tiled_kernel<T, COMP, false><<<bpg, tpb, Layout<T>::SMEM_BYTES, stream>>>(
             *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err, cfl, zc);
     if (launches)
         ++*launches;
     return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t
+set_smem(const void* fn, const size_t bytes)
+{
+    return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
 } // namespace
@@ -541,46 +1155,47 @@ ac_make_tensor_map(void* map_out, void* base, const Geom& g, const int precision
     return ac_encode_field_map(map_out, base, g, precision, hxp, HY);
 }
 
-/* Opts the kernel in to its dynamic shared memory on the current device; called
- * by acDeviceCreate, outside any stream capture. */
+/* Opts the kernels in to their dynamic shared memory on the current device;
+ * called by acDeviceCreate, outside any stream capture. */
 cudaError_t
 ac_solve_tiled_init(const int precision)
 {
-    /* both variants (with and without the upwinding terms) */
+    cudaError_t e;
     if (precision == 0) {
-        const cudaError_t e = cudaFuncSetAttribute(solve_tiled_kernel<double, false, false>,
-                                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                   (int)Layout<double>::SMEM_BYTES);
-        if (e != cudaSuccess)
+        typedef Layout<double> L;
+        if ((e = set_smem<double>((const void*)solve_tiled_kernel<double, false, false>,
+                                  L::SMEM_BYTES)) != cudaSuccess ||
+            (e = set_smem<double>((const void*)solve_tiled_kernel<double, false, true>,
+                                  L::SMEM_BYTES)) != cudaSuccess)
             return e;
-        return cudaFuncSetAttribute(solve_tiled_kernel<double, false, true>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)Layout<double>::SMEM_BYTES);
+        return set_smem<double>((const void*)solve_lead_kernel<double, false>,
+                                lead_smem_bytes<double>());
     }
-    const cudaError_t e = cudaFuncSetAttribute(solve_tiled_kernel<float, true, false>,
-                                               cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                               (int)Layout<float>::SMEM_BYTES);
-    if (e != cudaSuccess)
+    typedef Layout<float> L;
+    if ((e = set_smem<float>((const void*)solve_tiled_kernel<float, true, false>,
+                             L::SMEM_BYTES)) != cudaSuccess ||
+        (e = set_smem<float>((const void*)solve_tiled_kernel<float, true, true>, L::SMEM_BYTES)) !=
+            cudaSuccess)
         return e;
-    return cudaFuncSetAttribute(solve_tiled_kernel<float, true, true>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)Layout<float>::SMEM_BYTES);
+    return set_smem<float>((const void*)solve_lead_kernel<float, true>, lead_smem_bytes<float>());
 }
 
 cudaError_t
 ac_launch_solve_tiled64(const Geom& g, const void* tmap_in, const Fields64& f,
                         const StencilCoef& sc, const PhysConst& pc, const RkCoef& rk, int* err,
                         unsigned long long* cfl, cudaStream_t stream,
-                        unsigned long long* launches)
+                        unsigned long long* launches, const int kernel)
 {
-    return launch_tiled<double, false>(g, tmap_in, f, sc, pc, rk, err, cfl, stream, launches);
+    return launch_tiled<double, false>(g, tmap_in, f, sc, pc, rk, err, cfl, stream, launches,
+                                       kernel);
 }
 
 cudaError_t
 ac_launch_solve_tiled32(const Geom& g, const void* tmap_in, const Fields32& f,
                         const StencilCoef& sc, const PhysConst& pc, const RkCoef& rk, int* err,
                         unsigned long long* cfl, cudaStream_t stream,
-                        unsigned long long* launches)
+                        unsigned long long* launches, const int kernel)
 {
-    return launch_tiled<float, true>(g, tmap_in, f, sc, pc, rk, err, cfl, stream, launches);
+    return launch_tiled<float, true>(g, tmap_in, f, sc, pc, rk, err, cfl, stream, launches,
+                                     kernel);
 }

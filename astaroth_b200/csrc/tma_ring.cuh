@@ -15,6 +15,8 @@ namespace tma_ring {
 /* try_wait may suspend the thread for a short, implementation-defined time per
  * call; 2^22 calls bound a wait to seconds even if a copy never lands. */
 constexpr long long kWaitLimit = 1LL << 22;
+/* The bound under the fault-path test switch (a load that never lands). */
+constexpr long long kDebugWaitLimit = 1LL << 12;
 
 __device__ __forceinline__ uint32_t
 smem_addr(const void* p)
@@ -57,12 +59,28 @@ mbar_try_wait(uint64_t* bar, const unsigned parity)
 }
 
 __device__ __forceinline__ bool
-mbar_wait_bounded(uint64_t* bar, const unsigned parity)
+mbar_wait_bounded(uint64_t* bar, const unsigned parity, const long long limit = kWaitLimit)
 {
-    for (long long it = 0; it < kWaitLimit; ++it)
+    for (long long it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, parity))
             return true;
     return false;
+}
+
+/* Before a block exits: waits (bounded) until the last load issued into each of
+ * the ring's `ring` slots has landed, so that no copy into this block's shared
+ * memory is in flight even when an earlier wait gave up.  issued(s) is the
+ * number of loads issued into slot s; each completed one phase of its
+ * barrier. */
+template <typename F>
+__device__ __forceinline__ void
+drain_ring(uint64_t* bars, const int ring, F issued)
+{
+    for (int s = 0; s < ring; ++s) {
+        const int n = issued(s);
+        if (n > 0)
+            mbar_wait_bounded(&bars[s], (unsigned)((n - 1) & 1));
+    }
 }
 
 /* One box of the 4-D (x, y, z, field) map at (x, y, z, 0) into dst; x is in

@@ -29,6 +29,11 @@ aa ~ N(0, 1e-4^2)), nu = eta = 5e-3, cs = 1, gamma = 5/3, dt = 1e-3.
               state (AC_precision = 1): cell-updates/s, speed-up over FP64, and
               the per-field relative L-inf against the FP64 path after 100 steps
               from the same initial mesh (rank 0 at N=1).
+* cfl1024     the 1024^3 FP32-compensated run with adaptive CFL timesteps from the
+              on-device maxima (20 steps, ~149 GB), with the FP64 run on the same
+              dt sequence for its diagnostics (rank 0 at N=1).
+* adjoint     the 64^3 discrete-adjoint gradient through 200 steps: backward /
+              forward time (rank 0 at N=1).
 
 --impl reference times that CPU implementation alone, one bounded sample per
 step (rank 0; other ranks exit without work).  Multi-GPU runs are replicas:
@@ -70,6 +75,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32comp", action="store_true")
     ap.add_argument("--no-ensemble", action="store_true")
+    ap.add_argument("--no-cfl1024", action="store_true",
+                    help="skip the 1024^3 adaptive-CFL leg (about 149 GB of device memory)")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--workload", default="step512",
                     choices=["step512", "cfl1024", "adjoint64"],
                     help="step512: the FP64 RK3 step (default line); cfl1024: 1024^3 "
@@ -371,6 +379,20 @@ def run_gpu(args):
     if not args.no_ensemble:
         ens = ensemble_leg(args, torch, rank, world)
 
+    dev.destroy()
+    host = pinned = hmesh = None  # the host copies of the 512^3 mesh (17.8 GB) go first
+    cfl = adj = None
+    if rank == 0 and world == 1 and not args.no_cfl1024:
+        try:
+            cfl = cfl1024_leg()
+        except Exception as exc:  # reported, never fatal to the main line
+            cfl = {"error": str(exc)[:300]}
+    if rank == 0 and world == 1 and not args.no_adjoint:
+        try:
+            adj = adjoint_leg(max(3, min(args.steps, 10)), max(1, min(args.warmup, 3)))
+        except Exception as exc:
+            adj = {"error": str(exc)[:300]}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -398,12 +420,11 @@ def run_gpu(args):
                          "boundconds_ms_per_step": sum(bc_ms[-3:]),
                          "limiter": profile_limiter("solve_tiled_fp64_256.md")},
             "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
-            "fp32comp": fp32, "ensemble": ens,
+            "fp32comp": fp32, "ensemble": ens, "cfl1024": cfl, "adjoint": adj,
         }
         if fp32 and "ms_per_step" in fp32:
             fp32["speedup_vs_fp64"] = t_max / fp32["ms_per_step"]
         print(json.dumps(line), flush=True)
-    dev.destroy()
     adist.barrier()
     adist.destroy()
 
@@ -631,22 +652,22 @@ def diagnostics(dev):
 CFL1024_CDTV = 0.04
 
 
-def run_cfl1024(args):
-    """1024^3 interior, FP32 compensated (about 149 GB on the device), u a
-    solenoidal sum of 64 Fourier modes (|k| <= 8, amplitude 1e-2), aa ~
-    N(0, 1e-4^2), lnrho and s ~ U(-1e-5, 1e-5), seed 3; 20 RK3 steps whose dt
-    comes from the on-device CFL maxima (Courant factors cdt = 0.4 and
-    cdtv = CFL1024_CDTV).  The same run in FP64 with the same dt sequence checks
-    the diagnostics (max, min, rms of every field)."""
+def cfl1024_leg(n: int = 1024, steps: int = 20) -> dict:
+    """The 1024^3 FP32-compensated run with adaptive CFL timesteps: u a solenoidal
+    sum of 64 Fourier modes (|k| <= 8, amplitude 1e-2), aa ~ N(0, 1e-4^2), lnrho
+    and s ~ U(-1e-5, 1e-5), seed 3; 20 RK3 steps whose dt comes from the
+    on-device CFL maxima (Courant factors cdt = 0.4 and cdtv = CFL1024_CDTV).
+    The same run in FP64 with the same dt sequence checks the diagnostics (max,
+    min, rms of every field).  About 149 GB on the device, one run at a time."""
     import torch
     import astaroth_b200 as ab
 
-    n, steps = (args.n if args.n != 512 else 1024), 20
-    torch.cuda.set_device(0)
+    dev_id = torch.cuda.current_device()
     res = {}
+    dts = []
     for prec in (1, 0):
         info = ab.make_info(n, precision=prec, cdtv=CFL1024_CDTV, **ab.CONFIG_PARAMS)
-        dev = ab.Device(info)
+        dev = ab.Device(info, device_id=dev_id)
         t0 = time.perf_counter()
         load_fields_by_parts(ab, dev, info, 3)
         t_load = time.perf_counter() - t0
@@ -654,11 +675,10 @@ def run_cfl1024(args):
         free_b, total_b = torch.cuda.mem_get_info()
         if prec == 1:
             dev.calc_timestep()
-            dts = []
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
         l0 = dev.launch_count()
-        with ClockSampler(0) as clk:
+        with ClockSampler(dev_id) as clk:
             ev0.record(stream)
             for s in range(steps):
                 if prec == 1:
@@ -682,29 +702,40 @@ def run_cfl1024(args):
            for k in d32}
     peak, _ = peaks()
     achieved = BYTES_PER_CELL_STEP["fp32comp"] * n ** 3 / (res[1]["ms_per_step"] * 1e-3) / 1e9
-    line = {"metric": f"cell-updates/s per RK3 step at {n}^3 (FP32-compensated, adaptive CFL)",
-            "value": res[1]["value"], "unit": UNIT, "n_gpus": 1, "steps": steps, "warmup": 0,
-            "ms_per_step": res[1]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32 (compensated hi/lo)",
+    return {"metric": f"cell-updates/s per RK3 step at {n}^3 (FP32-compensated, adaptive CFL)",
+            "value": res[1]["value"], "unit": UNIT, "steps": steps,
+            "ms_per_step": res[1]["ms_per_step"], "dtype": "f32 (compensated hi/lo)",
             "data": "synthetic (seed 3: solenoidal uu of 64 modes, |k|<=8, amplitude 1e-2; "
                     "aa ~ N(0,1e-4^2); lnrho, s ~ U(-1e-5,1e-5))",
-            "config": {"workload": f"{n}^3 FP32-compensated, {steps} RK3 steps, dt from the "
-                                   f"on-device CFL maxima each step (cdt=0.4, "
-                                   f"cdtv={CFL1024_CDTV})", "n": n},
+            "workload": f"{n}^3 FP32-compensated, {steps} RK3 steps, dt from the on-device CFL "
+                        f"maxima each step (cdt=0.4, cdtv={CFL1024_CDTV})",
             "dt": dts, "gpu_launches": res[1]["gpu_launches"], "clocks": res[1]["clocks"],
-            "device_bytes_used": res[1]["device_bytes_used"],
+            "device_bytes_used": res[1]["device_bytes_used"], "load_s": res[1]["load_s"],
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "note": "whole step incl. halo fills and "
                                                           "the per-step host read of dt"},
             "fp64_same_dts": {"ms_per_step": res[0]["ms_per_step"], "value": res[0]["value"],
-                              "device_bytes_used": res[0]["device_bytes_used"]},
+                              "device_bytes_used": res[0]["device_bytes_used"],
+                              "clocks": res[0]["clocks"]},
             "diagnostics_fp32comp": d32, "diagnostics_fp64": d64,
             "diagnostics_rel_diff_vs_fp64": rel,
             "diagnostics_max_rel_diff": max(rel.values())}
+
+
+def run_cfl1024(args):
+    """--workload cfl1024: the 1024^3 leg alone, as its own line."""
+    import torch
+    torch.cuda.set_device(0)
+    d = cfl1024_leg(args.n if args.n != 512 else 1024)
+    line = {k: d[k] for k in ("metric", "value", "unit", "steps", "ms_per_step", "dtype",
+                              "data")}
+    line.update({"n_gpus": 1, "warmup": 0, "higher_is_better": True, "scaling": "weak",
+                 "vs_baseline": None, "config": {"workload": d["workload"]}})
+    line.update({k: v for k, v in d.items() if k not in line})
     print(json.dumps(line), flush=True)
 
 
-def run_adjoint64(args):
+def adjoint_leg(steps_timed: int, warmup: int) -> dict:
     """Gradient of J = E_kin + E_mag after 200 FP64 RK3 steps at 64^3 (dt = 1e-3,
     seed 4, checkpoints every 20 steps) with respect to the initial fields and
     nu, eta, through the torch.autograd wrapper over the C ABI: forward time,
@@ -715,13 +746,13 @@ def run_adjoint64(args):
     from astaroth_b200 import autograd as AG
 
     n, steps, every, dt = 64, 200, 20, 1e-3
-    torch.cuda.set_device(0)
     info = ab.make_info(n, **ab.CONFIG_PARAMS)
     f = torch.from_numpy(ab.seeded_mesh(info, 4)).cuda()
-    dev = ab.Device(info)
+    dev = ab.Device(info, device_id=torch.cuda.current_device())
     fwd, bwd = [], []
     l0 = dev.launch_count()
-    for it in range(args.warmup + args.steps):
+    peak_bytes = 0
+    for it in range(warmup + steps_timed):
         x0 = f.clone().requires_grad_(True)
         nu = torch.tensor(5e-3, dtype=torch.float64, device="cuda", requires_grad=True)
         eta = torch.tensor(5e-3, dtype=torch.float64, device="cuda", requires_grad=True)
@@ -735,24 +766,34 @@ def run_adjoint64(args):
         J.backward()
         e[2].record()
         torch.cuda.synchronize()
-        if it >= args.warmup:
+        peak_bytes = max(peak_bytes, torch.cuda.max_memory_allocated())
+        if it >= warmup:
             fwd.append(e[0].elapsed_time(e[1]))
             bwd.append(e[1].elapsed_time(e[2]))
     launches = dev.launch_count() - l0
     dev.destroy()
     tf, tb = statistics.median(fwd), statistics.median(bwd)
-    line = {"metric": "adjoint cost: backward (recompute + reverse sweep) / forward time",
-            "value": tb / tf, "unit": "x", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seed 4, benchmark "
-            "distributions)",
-            "config": {"workload": f"{n}^3, {steps} RK3 steps, dt={dt}, checkpoints every "
-                                   f"{every} steps, J = E_kin + E_mag at the final time",
-                       "n": n},
-            "forward_ms": tf, "backward_ms": tb,
+    return {"metric": "adjoint cost: backward (recompute + reverse sweep) / forward time",
+            "value": tb / tf, "unit": "x", "higher_is_better": False, "dtype": "f64",
+            "workload": f"{n}^3, {steps} RK3 steps, dt={dt}, checkpoints every {every} steps, "
+                        f"J = E_kin + E_mag at the final time; gradients w.r.t. the 8 initial "
+                        f"fields and nu, eta",
+            "samples": steps_timed, "forward_ms": tf, "backward_ms": tb,
             "forward_ms_per_step": tf / steps, "backward_ms_per_step": tb / steps,
-            "peak_torch_bytes": torch.cuda.max_memory_allocated(),
-            "gpu_launches": launches}
+            "peak_torch_bytes": peak_bytes, "gpu_launches": launches}
+
+
+def run_adjoint64(args):
+    """--workload adjoint64: the adjoint leg alone, as its own line."""
+    import torch
+    torch.cuda.set_device(0)
+    d = adjoint_leg(args.steps, args.warmup)
+    line = {"metric": d["metric"], "value": d["value"], "unit": "x", "n_gpus": 1,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seed 4, benchmark distributions)",
+            "config": {"workload": d["workload"], "n": 64}}
+    line.update({k: v for k, v in d.items() if k not in line})
     print(json.dumps(line), flush=True)
 
 

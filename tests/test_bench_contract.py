@@ -65,7 +65,7 @@ def test_reference_arm_maps_no_product_library():
 
 @pytest.mark.gpu
 def test_gpu_line_small():
-    d = _run(["--n", "64", "--steps", "2", "--warmup", "3", "--no-ensemble",
+    d = _run(["--n", "64", "--steps", "2", "--warmup", "3", "--no-ensemble", "--no-cfl1024",
               "--accuracy-steps", "2"], timeout=900)
     _check_base(d)
     assert d["n_gpus"] == 1 and d["steps"] == 2 and d["warmup"] == 3
@@ -79,3 +79,5 @@ def test_gpu_line_small():
     assert {"sm_mhz", "sm_max_mhz", "reasons"} <= set(c)
     assert d["cpu_baseline"]["value"] > 0
     assert d["fp32comp"]["rel_linf_vs_fp64"]["max"] <= 1e-5
+    a = d["adjoint"]
+    assert a["value"] > 0 and a["forward_ms"] > 0 and a["backward_ms"] > 0

@@ -46,10 +46,13 @@ def case(name):
     return info, ab.seeded_mesh(info, c["seed"])
 
 
-def gpu_run(info, f0, dt, nsteps, graph=False, plain=False):
+def gpu_run(info, f0, dt, nsteps, graph=False, plain=False, kernel=None):
+    """kernel: AC_debug_plain_kernel (0 default tiled, 1 plain, 2 per-plane taps)"""
     with ab.Device(info) as dev:
         if plain:
             dev.set_int(capi.IntParam.AC_debug_plain_kernel, 1)
+        if kernel is not None:
+            dev.set_int(capi.IntParam.AC_debug_plain_kernel, kernel)
         dev.load_mesh(f0)
         for _ in range(nsteps):
             if graph:
@@ -185,13 +188,32 @@ def test_graph_step_equals_loop_bitwise():
     assert np.array_equal(oracle.interior(a), oracle.interior(b))
 
 
-def test_plain_and_tiled_kernels_agree():
-    info = ab.make_info((64, 40, 24), **ab.CONFIG_PARAMS)
-    f = ab.seeded_mesh(info, 6)
-    a = gpu_run(info, f, 1e-3, 2, plain=True)
-    b = gpu_run(info, f, 1e-3, 2, plain=False)
-    err = oracle.rel_linf(a, b)
-    assert err.max() <= 1e-13, err
+@pytest.mark.parametrize("n", [(64, 40, 24), (66, 14, 37), (96, 8, 150)])
+def test_plain_and_tiled_kernels_agree(n):
+    """The plain kernel, the per-plane tap kernel and the default leading-plane
+    kernel (tensor-memory delay line, separable xz/yz mixed derivatives): partial
+    tiles in x and y, z extents that split into uneven chunks."""
+    info = ab.make_info(n, **ab.CONFIG_PARAMS)
+    f = ab.seeded_mesh(info, 6, amp_scalar=0.05, sigma_uu=0.05, sigma_aa=0.02)
+    a = gpu_run(info, f, 1e-3, 2, kernel=1)
+    b = gpu_run(info, f, 1e-3, 2, kernel=0)
+    c = gpu_run(info, f, 1e-3, 2, kernel=2)
+    for cand in (b, c):
+        err = oracle.rel_linf(cand, a)
+        assert err.max() <= 1e-13, err
+
+
+def test_leading_plane_kernel_vs_oracle_3_steps():
+    """The default kernel against the CPU oracle on a mesh with several z
+    chunks per column and partial x/y tiles."""
+    n = (66, 14, 37)
+    info = ab.make_info(n, **ab.CONFIG_PARAMS)
+    f = ab.seeded_mesh(info, 8, amp_scalar=0.05, sigma_uu=0.05, sigma_aa=0.02)
+    got = gpu_run(info, f, 1e-3, 3, kernel=0)
+    ref = f.copy()
+    oracle.integrate(ref, ab.info_to_dict(info), 1e-3, 3, "port")
+    err = oracle.rel_linf(got, ref)
+    assert err.max() <= 1e-12, err
 
 
 # ---------------------------------------------------------------- reductions
