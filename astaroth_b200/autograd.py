@@ -19,6 +19,7 @@ interior; the returned gradient is zero on the halo cells.
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 
 import torch
@@ -41,23 +42,70 @@ def _d1(f, axis, inv_ds):
     return out * inv_ds
 
 
-def energy(fields: torch.Tensor, info) -> torch.Tensor:
-    """J = sum over the interior of (1/2) exp(lnrho) |u|^2 dV + |curl A|^2 / (2 mu0) dV,
-    with the same 6th-order first derivatives as the solver (periodic box)."""
+def energy_density(fields: torch.Tensor, info) -> torch.Tensor:
+    """Per-cell terms of J over the interior: (1/2) exp(lnrho) |u|^2 dV +
+    |curl A|^2 / (2 mu0) dV, with the same 6th-order first derivatives as the
+    solver (periodic box).  Differences of J between nearby states are best
+    formed cell by cell from these, before the sum."""
     q = interior(fields)
     ds = info.real3_params[capi.Real3Param.AC_ds]
     inv = (1.0 / ds.x, 1.0 / ds.y, 1.0 / ds.z)
     dV = ds.x * ds.y * ds.z
     mu0 = info.real_params[capi.RealParam.AC_mu0]
     lnrho, u, a = q[0], q[1:4], q[4:7]
-    ekin = 0.5 * (torch.exp(lnrho) * (u * u).sum(0)).sum() * dV
+    ekin = 0.5 * (torch.exp(lnrho) * (u * u).sum(0)) * dV
     # axes of a field: (z, y, x) -> x = 2, y = 1, z = 0
     g = [[_d1(a[c], 2, inv[0]), _d1(a[c], 1, inv[1]), _d1(a[c], 0, inv[2])] for c in range(3)]
     bx = g[2][1] - g[1][2]
     by = g[0][2] - g[2][0]
     bz = g[1][0] - g[0][1]
-    emag = ((bx * bx + by * by + bz * bz).sum() / (2.0 * mu0)) * dV
+    emag = (bx * bx + by * by + bz * bz) / (2.0 * mu0) * dV
     return ekin + emag
+
+
+class _Energy(torch.autograd.Function):
+    """J and dJ/dfields by the library's energy kernels (acEnergyFunctional)."""
+
+    @staticmethod
+    def forward(ctx, fields, info):
+        lib = capi.load()
+        f = fields.detach().contiguous()
+        scratch = torch.empty(lib.acEnergyFunctionalScratchBytes(info) // 8 + 1,
+                              dtype=torch.float64, device=f.device)
+        J = torch.empty((), dtype=torch.float64, device=f.device)
+        ptrs = (C.c_void_p * 8)(*[f[q].data_ptr() for q in range(8)])
+        stream = torch.cuda.current_stream(f.device).cuda_stream
+        if lib.acEnergyFunctional(info, ptrs, C.c_void_p(J.data_ptr()), None,
+                                  C.c_void_p(scratch.data_ptr()), C.c_void_p(stream)) != 0:
+            raise AstarothError("acEnergyFunctional failed")
+        ctx.save_for_backward(f)
+        ctx.info = info
+        return J
+
+    @staticmethod
+    def backward(ctx, gJ):
+        (f,) = ctx.saved_tensors
+        lib = capi.load()
+        scratch = torch.empty(lib.acEnergyFunctionalScratchBytes(ctx.info) // 8 + 1,
+                              dtype=torch.float64, device=f.device)
+        J = torch.empty((), dtype=torch.float64, device=f.device)
+        grad = torch.zeros_like(f)
+        fp = (C.c_void_p * 8)(*[f[q].data_ptr() for q in range(8)])
+        gp = (C.c_void_p * 8)(*[grad[q].data_ptr() for q in range(8)])
+        stream = torch.cuda.current_stream(f.device).cuda_stream
+        if lib.acEnergyFunctional(ctx.info, fp, C.c_void_p(J.data_ptr()), gp,
+                                  C.c_void_p(scratch.data_ptr()), C.c_void_p(stream)) != 0:
+            raise AstarothError("acEnergyFunctional failed")
+        return grad * gJ, None
+
+
+def energy(fields: torch.Tensor, info) -> torch.Tensor:
+    """J = sum over the interior of (1/2) exp(lnrho) |u|^2 dV + |curl A|^2 / (2 mu0) dV,
+    with the same 6th-order first derivatives as the solver (periodic box); on a
+    CUDA tensor by the library's kernels (value and gradient), else in torch."""
+    if fields.is_cuda:
+        return _Energy.apply(fields, info)
+    return energy_density(fields, info).sum()
 
 
 class _Integrate(torch.autograd.Function):

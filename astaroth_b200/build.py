@@ -30,7 +30,7 @@ CC_FLAGS = ["-O2", "-fPIC", "-fopenmp", "-std=c11", "-Wall", f"-I{INCLUDE}"]
 
 CU_SOURCES = ["device.cu", "device_data.cu", "device_adjoint.cu", "solve.cu", "solve_tiled.cu",
               "boundconds.cu", "reduce.cu", "cfl.cu", "adjoint.cu", "ensemble.cu", "forcing.cu",
-              "bfield.cu"]
+              "bfield.cu", "energy.cu"]
 C_SOURCES = ["host.c"]
 HEADERS = ["internal.h", "mhd_rhs.cuh", "mhd_rhs_adjoint.cuh", "stencil_plain.cuh", "solve_cell.cuh",
            "halo.cuh", "tma_ring.cuh", "tmem.cuh", "device_impl.h"]

@@ -318,6 +318,9 @@ SIGNATURES = {
     "acDeviceGetStreamHandle": (C.c_void_p, [Device_p, C.c_int]),
     "acDeviceGetLaunchCount": (C.c_ulonglong, [Device_p]),
     "acDeviceDebugSkipPlaneLoad": (C.c_int, [Device_p, C.c_int]),
+    "acEnergyFunctional": (C.c_int, [AcMeshInfo, C.POINTER(C.c_void_p), C.c_void_p,
+                                     C.POINTER(C.c_void_p), C.c_void_p, C.c_void_p]),
+    "acEnergyFunctionalScratchBytes": (C.c_size_t, [AcMeshInfo]),
     "acB200Version": (C.c_char_p, []),
     "acReduceNoAlloc": (C.c_int, [C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_int, C.c_int,
                                   AcReduction, C.c_void_p, C.c_int, C.c_void_p]),

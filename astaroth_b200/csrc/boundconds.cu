@@ -12,9 +12,13 @@
  * follows the host model on all grids.
  *
  * One launch fills all requested arrays (the reference launches once per
- * field, src/core/device.cc:999-1017).  For the whole-mesh box the threads
- * enumerate only the ghost cells (z slabs, then y slabs, then x slabs), so
- * no thread is spent on the interior.
+ * field, src/core/device.cc:999-1017).  The whole-mesh fill works by rows
+ * (x lines): a row with a ghost y or z index is copied whole, by one warp with
+ * coalesced accesses, from the row it wraps to, with the x wrap at both ends;
+ * a row of the interior (y, z) gets its six x ghosts from one thread.
+ * Every source is an interior cell, so no ghost reads another ghost and the
+ * order does not matter.  Index arithmetic is 32-bit without divisions by a
+ * 64-bit value.
  */
 #include "internal.h"
 #include "halo.cuh"
@@ -43,18 +47,78 @@ copy_wrapped(const Geom& g, const ArrayList<T>& fl, const int i, const int j, co
             fl.p[q][dst] = fl.p[q][src];
 }
 
-/* Whole mesh: t enumerates the ghost cells only. */
+/* Whole mesh by rows.  Blocks [0, blocks_rows) copy the ghost rows, one warp
+ * per row; the others fill the six x ghosts of the interior rows, one thread
+ * per row.  Sources (interior cells) and destinations (ghost cells) never
+ * overlap, so each thread issues its loads before its stores.  blockIdx.y is
+ * the array. */
 template <typename T>
-__global__ void
-periodic_halo_kernel(const Geom g, const ArrayList<T> fl, const long long nzs,
-                     const long long nys, const long long total)
+__global__ void __launch_bounds__(256)
+periodic_rows_kernel(const Geom g, const ArrayList<T> fl, const int blocks_rows)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= total)
-        return;
-    int i, j, k;
-    halo_cell(g, t, nzs, nys, i, j, k);
-    copy_wrapped(g, fl, i, j, k);
+    T* a         = fl.p[blockIdx.y];
+    const int nx = g.nx, ny = g.ny, nz = g.nz, mx = g.mx, my = g.my;
+    if ((int)blockIdx.x < blocks_rows) {
+        /* ghost rows: the 6 ghost z planes (my rows each), then the 6 ghost y
+         * rows of each interior z plane */
+        const int r    = (int)blockIdx.x * 8 + (int)(threadIdx.x >> 5);
+        const int lane = threadIdx.x & 31;
+        if (r >= 6 * (my + nz))
+            return;
+        int j, k;
+        if (r < 6 * my) {
+            const int kk = r / my;
+            j            = r - kk * my;
+            k            = kk < NGHOST ? kk : nz + kk;
+        }
+        else {
+            const int u  = r - 6 * my;
+            const int jj = u % 6;
+            k            = NGHOST + u / 6;
+            j            = jj < NGHOST ? jj : ny + jj;
+        }
+        const int js = (j - NGHOST + ny) % ny + NGHOST;
+        const int ks = (k - NGHOST + nz) % nz + NGHOST;
+        T* dst       = a + geom_idx(g, 0, j, k);
+        const T* src = a + geom_idx(g, 0, js, ks);
+        constexpr int B = 8; /* loads in flight per lane */
+        for (int x0 = lane; x0 < mx; x0 += 32 * B) {
+            T v[B];
+#pragma unroll
+            for (int u = 0; u < B; ++u) {
+                const int x  = x0 + 32 * u;
+                const int xs = x < NGHOST ? x + nx : x >= nx + NGHOST ? x - nx : x;
+                v[u]         = x < mx ? src[xs] : T(0);
+            }
+#pragma unroll
+            for (int u = 0; u < B; ++u) {
+                const int x = x0 + 32 * u;
+                if (x < mx)
+                    dst[x] = v[u];
+            }
+        }
+    }
+    else {
+        /* the six x ghosts of interior row (j, k): x = 0..2 <- nx..nx+2 and
+         * x = nx+3..nx+5 <- 3..5 */
+        const int row = ((int)blockIdx.x - blocks_rows) * 256 + (int)threadIdx.x;
+        if (row >= ny * nz)
+            return;
+        const int k = NGHOST + row / ny;
+        const int j = NGHOST + row - (row / ny) * ny;
+        T* rp       = a + geom_idx(g, 0, j, k);
+        T v[6];
+#pragma unroll
+        for (int c = 0; c < NGHOST; ++c) {
+            v[c]          = rp[nx + c];
+            v[NGHOST + c] = rp[NGHOST + c];
+        }
+#pragma unroll
+        for (int c = 0; c < NGHOST; ++c) {
+            rp[c]               = v[c];
+            rp[nx + NGHOST + c] = v[NGHOST + c];
+        }
+    }
 }
 
 /* General box [start, end): interior cells are skipped. */
@@ -245,11 +309,14 @@ ac_launch_periodic(const Geom& g, T* const* arrays, const int n, const Volume st
     const bool whole = start.x == 0 && start.y == 0 && start.z == 0 && end.x == (size_t)g.mx &&
                        end.y == (size_t)g.my && end.z == (size_t)g.mz;
     if (whole) {
-        long long nzs, nys;
-        const long long total = halo_count(g, &nzs, &nys);
-        const int tpb         = 256;
-        const long long bpg   = (total + tpb - 1) / tpb;
-        periodic_halo_kernel<T><<<(unsigned)bpg, tpb, 0, stream>>>(g, fl, nzs, nys, total);
+        const long long ghost_rows = 6LL * (g.my + g.nz);
+        const long long irows      = (long long)g.ny * g.nz;
+        const long long b_rows     = (ghost_rows + 7) / 8;
+        const long long b_cells    = (irows + 255) / 256;
+        if (b_rows + b_cells > 0x7fffffffLL)
+            return cudaErrorInvalidValue;
+        periodic_rows_kernel<T><<<dim3((unsigned)(b_rows + b_cells), (unsigned)n), 256, 0,
+                                  stream>>>(g, fl, (int)b_rows);
     }
     else {
         const int3 s = make_int3((int)start.x, (int)start.y, (int)start.z);

@@ -88,6 +88,7 @@ ac_make_phys(const AcMeshInfo& info, PhysConst* pc)
     pc->K            = r[AC_K_heatcond];
     pc->upwind       = info.int_params[AC_upwind] != 0;
     pc->debug_skip_load = 0;
+    pc->cfl_sum         = info.int_params[AC_additive_timestep] != 0;
     pc->forcing      = 0;
     for (int a = 0; a < 3; ++a)
         pc->f_k[a] = pc->f_re[a] = pc->f_im[a] = 0.0;
@@ -98,13 +99,19 @@ ac_make_phys(const AcMeshInfo& info, PhysConst* pc)
 
 /* The forcing of a substep-2 launch (mhdsolver.ac:531-541): active when
  * AC_lforcing is set and AC_current_time > AC_switch_forcing. */
-/* AC_debug_plain_kernel: 0 = the leading-plane tiled kernel (default), 1 = the
- * plain kernel, 2 = the per-plane tap tiled kernel */
+/* AC_debug_plain_kernel: 0 = the automatic tiled choice (default), 1 = the plain
+ * kernel, 2 = the per-plane tap tiled kernel, 3 = the leading-plane kernel,
+ * 4 = the leading-plane kernel with the other group exchange */
 static int
 solve_variant_of(const AcMeshInfo& info)
 {
-    const int v = info.int_params[AC_debug_plain_kernel];
-    return v == 1 ? 0 : v == 2 ? AC_SOLVE_TILED_TAPS : AC_SOLVE_TILED_LEAD;
+    switch (info.int_params[AC_debug_plain_kernel]) {
+    case 1: return 0;
+    case 2: return AC_SOLVE_TILED_TAPS;
+    case 3: return AC_SOLVE_TILED_LEAD;
+    case 4: return AC_SOLVE_TILED_LEAD_ALT;
+    default: return AC_SOLVE_TILED_AUTO;
+    }
 }
 
 static void
@@ -192,6 +199,7 @@ release(Device d)
     cudaFree(d->adj_mu);
     cudaFree(d->adj_pgrad);
     cudaFree(d->adj_tape);
+    cudaFree(d->adj_state);
     cudaFree(d->bfield);
     cudaFree(d->stage);
     if (d->stage_loaded)

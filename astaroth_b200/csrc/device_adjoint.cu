@@ -15,13 +15,35 @@
 
 /* ---- discrete adjoint ---- */
 
+/* The adjoint works in FP64 on the host layout (row pitch mx) for both
+ * precisions: on an FP32-compensated device the forward states it linearises
+ * about are the (hi, lo) pairs joined to doubles, and the reverse sweep, its
+ * inner products and the parameter adjoints are FP64. */
+static Geom
+adj_geom(const Device d)
+{
+    return ac_make_geom(d->config, 0);
+}
+
+/* The 8 in-buffers of an FP32-compensated device joined to doubles in the
+ * host layout, field q at q * cells of dst. */
+static cudaError_t
+join_state(const Device d, cudaStream_t st, double* dst, unsigned long long* launches)
+{
+    const Geom g64 = adj_geom(d);
+    for (int q = 0; q < AC_NF; ++q) {
+        const int b          = d->in_idx[q];
+        const cudaError_t e  = ac_launch_join(d->geom, arr_hi(d, b, q), arr_lo(d, b, q),
+                                              dst + (size_t)q * g64.cells, st, launches);
+        if (e != cudaSuccess)
+            return e;
+    }
+    return cudaSuccess;
+}
+
 static AcResult
 ensure_adjoint(const Device d)
 {
-    if (d->precision != 0) {
-        fprintf(stderr, "astaroth_b200: the adjoint needs an FP64 device (AC_precision = 0)\n");
-        return AC_FAILURE;
-    }
     if (d->config.int_params[AC_upwind]) {
         /* |u| in the upwinding terms has no derivative at u = 0; the reverse
          * pass covers the equations without them */
@@ -30,12 +52,14 @@ ensure_adjoint(const Device d)
     }
     if (d->adj_lf)
         return AC_SUCCESS;
-    const size_t fb = (size_t)d->geom.cells * sizeof(double);
+    const size_t fb = (size_t)adj_geom(d).cells * sizeof(double);
     AC_CUDA_CHECK(cudaMalloc((void**)&d->adj_lf, AC_NF * fb));
     AC_CUDA_CHECK(cudaMalloc((void**)&d->adj_lw, AC_NF * fb));
     AC_CUDA_CHECK(cudaMalloc((void**)&d->adj_mu, AC_MU_COUNT * fb));
     AC_CUDA_CHECK(cudaMalloc((void**)&d->adj_pgrad, 2 * sizeof(double)));
     AC_CUDA_CHECK(cudaMemset(d->adj_mu, 0, AC_MU_COUNT * fb));
+    if (d->precision != 0) /* the joined in-buffers of a per-substep adjoint call */
+        AC_CUDA_CHECK(cudaMalloc((void**)&d->adj_state, AC_NF * fb));
     return AC_SUCCESS;
 }
 
@@ -47,14 +71,15 @@ acDeviceLoadAdjoint(const Device d, const Stream stream, const AcReal* const* la
     AC_CUDA_CHECK(cudaSetDevice(d->id));
     if (ensure_adjoint(d) != AC_SUCCESS)
         return AC_FAILURE;
-    cudaStream_t st = d->streams[stream];
-    const size_t fb = (size_t)d->geom.cells * sizeof(double);
+    cudaStream_t st   = d->streams[stream];
+    const size_t cells = (size_t)adj_geom(d).cells;
+    const size_t fb   = cells * sizeof(double);
     for (int q = 0; q < AC_NF; ++q) {
         if (lam_f && lam_f[q])
-            AC_CUDA_CHECK(cudaMemcpyAsync(d->adj_lf + (size_t)q * d->geom.cells, lam_f[q], fb,
+            AC_CUDA_CHECK(cudaMemcpyAsync(d->adj_lf + (size_t)q * cells, lam_f[q], fb,
                                           cudaMemcpyDeviceToDevice, st));
         else
-            AC_CUDA_CHECK(cudaMemsetAsync(d->adj_lf + (size_t)q * d->geom.cells, 0, fb, st));
+            AC_CUDA_CHECK(cudaMemsetAsync(d->adj_lf + (size_t)q * cells, 0, fb, st));
     }
     AC_CUDA_CHECK(cudaMemsetAsync(d->adj_lw, 0, AC_NF * fb, st));
     AC_CUDA_CHECK(cudaMemsetAsync(d->adj_pgrad, 0, 2 * sizeof(double), st));
@@ -67,10 +92,11 @@ acDeviceStoreAdjoint(const Device d, const Stream stream, AcReal* const* lam_f)
     if (!d || !lam_f || !stream_ok(stream) || !d->adj_lf)
         return AC_FAILURE;
     AC_CUDA_CHECK(cudaSetDevice(d->id));
-    const size_t fb = (size_t)d->geom.cells * sizeof(double);
+    const size_t cells = (size_t)adj_geom(d).cells;
+    const size_t fb    = cells * sizeof(double);
     for (int q = 0; q < AC_NF; ++q)
         if (lam_f[q])
-            AC_CUDA_CHECK(cudaMemcpyAsync(lam_f[q], d->adj_lf + (size_t)q * d->geom.cells, fb,
+            AC_CUDA_CHECK(cudaMemcpyAsync(lam_f[q], d->adj_lf + (size_t)q * cells, fb,
                                           cudaMemcpyDeviceToDevice, d->streams[stream]));
     return AC_SUCCESS;
 }
@@ -85,18 +111,25 @@ launch_adjoint(const Device d, cudaStream_t st, const int step, const double dt,
     PhysConst pc;
     ac_make_stencil(d->config, &sc);
     ac_make_phys(d->config, &pc);
+    const Geom g = adj_geom(d);
+    if (!state && d->precision != 0) {
+        const cudaError_t e = join_state(d, st, d->adj_state, &d->launches);
+        if (e != cudaSuccess)
+            return e;
+        state = d->adj_state;
+    }
     AdjointFields a;
     for (int q = 0; q < AC_NF; ++q) {
-        a.f[q]  = state ? state + (size_t)q * d->geom.cells : arr64(d, d->in_idx[q], q);
-        a.lf[q] = d->adj_lf + (size_t)q * d->geom.cells;
-        a.lw[q] = d->adj_lw + (size_t)q * d->geom.cells;
+        a.f[q]  = state ? state + (size_t)q * g.cells : arr64(d, d->in_idx[q], q);
+        a.lf[q] = d->adj_lf + (size_t)q * g.cells;
+        a.lw[q] = d->adj_lw + (size_t)q * g.cells;
     }
     for (int m = 0; m < AC_MU_COUNT; ++m)
-        a.mu[m] = d->adj_mu + (size_t)m * d->geom.cells;
+        a.mu[m] = d->adj_mu + (size_t)m * g.cells;
     const double alpha[3] = {0.0, -5.0 / 9.0, -153.0 / 128.0};
     const double beta[3]  = {1.0 / 3.0, 15.0 / 16.0, 8.0 / 15.0};
-    return ac_launch_adjoint_substep(d->geom, a, sc, pc, alpha[step], beta[step], dt,
-                                     d->adj_pgrad, st, &d->launches);
+    return ac_launch_adjoint_substep(g, a, sc, pc, alpha[step], beta[step], dt, d->adj_pgrad,
+                                     st, &d->launches);
 }
 
 extern "C" AcResult
@@ -121,7 +154,7 @@ acDeviceIntegrateSubstepAdjoint(const Device d, const Stream stream, const int s
 static cudaError_t
 record_tape(Device d, cudaStream_t st, const int steps, const double dt)
 {
-    const size_t state_elems = (size_t)AC_NF * d->geom.cells;
+    const size_t state_elems = (size_t)AC_NF * adj_geom(d).cells;
     const Volume m0          = {0, 0, 0};
     const Volume m1          = {(size_t)d->geom.mx, (size_t)d->geom.my, (size_t)d->geom.mz};
     for (int n = 0; n < steps; ++n)
@@ -129,10 +162,13 @@ record_tape(Device d, cudaStream_t st, const int steps, const double dt)
             cudaError_t e = launch_periodic(d, st, 0, AC_NF, m0, m1, NULL);
             if (e != cudaSuccess)
                 return e;
-            /* the 8 in-buffers are one contiguous block: one copy per state */
-            e = ac_launch_copy(arr64(d, d->in_idx[0], 0),
-                               d->adj_tape + (size_t)(3 * n + s) * state_elems,
-                               (long long)state_elems, st, NULL);
+            double* slot = d->adj_tape + (size_t)(3 * n + s) * state_elems;
+            /* FP64: the 8 in-buffers are one contiguous block, one copy per state;
+             * FP32 compensated: (hi, lo) joined to doubles */
+            e = d->precision == 0
+                    ? ac_launch_copy(arr64(d, d->in_idx[0], 0), slot, (long long)state_elems, st,
+                                     NULL)
+                    : join_state(d, st, slot, NULL);
             if (e != cudaSuccess)
                 return e;
             e = launch_substep(d, st, s, dt, NULL);
@@ -156,7 +192,7 @@ acDeviceAdjointTapeForward(const Device d, const Stream stream, const int steps,
     AC_CUDA_CHECK(cudaSetDevice(d->id));
     if (ensure_adjoint(d) != AC_SUCCESS)
         return AC_FAILURE;
-    const size_t state_elems = (size_t)AC_NF * d->geom.cells;
+    const size_t state_elems = (size_t)AC_NF * adj_geom(d).cells;
     if (d->adj_tape_states < 3 * steps) {
         AC_CUDA_CHECK(cudaDeviceSynchronize());
         invalidate_tape_graph(d);
@@ -192,7 +228,7 @@ acDeviceAdjointTapeForward(const Device d, const Stream stream, const int steps,
         d->tape_stream[blk] = (int)stream;
     }
     AC_CUDA_CHECK(cudaGraphLaunch(d->tape_exec[blk], st));
-    d->launches += 9ull * steps;
+    d->launches += (d->precision == 0 ? 9ull : 33ull) * steps; /* FP32: 8 joins per state */
     d->out_set = 0;
     if ((3 * steps) & 1) /* three swaps per step */
         acDeviceSwapBuffers(d);
@@ -216,7 +252,7 @@ acDeviceAdjointTapeBackward(const Device d, const Stream stream, const int steps
         return AC_FAILURE;
     AC_CUDA_CHECK(cudaSetDevice(d->id));
     cudaStream_t st             = d->streams[stream];
-    const size_t state_elems    = (size_t)AC_NF * d->geom.cells;
+    const size_t state_elems    = (size_t)AC_NF * adj_geom(d).cells;
     for (int n = steps - 1; n >= 0; --n)
         for (int s = 2; s >= 0; --s)
             AC_CUDA_CHECK(launch_adjoint(d, st, s, dt,

@@ -415,13 +415,13 @@ record_members(Ensemble e, const int s0, const int s1, unsigned long long* launc
             if constexpr (COMP)
                 err = e->tiled[m] ? ac_launch_solve_tiled32(r.g, tmap, f, e->sc[m], e->pc[m], rk,
                                                             e->err, nullptr, st, launches,
-                                                            AC_SOLVE_TILED_LEAD)
+                                                            AC_SOLVE_TILED_AUTO)
                                   : ac_launch_solve_plain32(r.g, f, e->sc[m], e->pc[m], rk, nullptr,
                                                             st, launches);
             else
                 err = e->tiled[m] ? ac_launch_solve_tiled64(r.g, tmap, f, e->sc[m], e->pc[m], rk,
                                                             e->err, nullptr, st, launches,
-                                                            AC_SOLVE_TILED_LEAD)
+                                                            AC_SOLVE_TILED_AUTO)
                                   : ac_launch_solve_plain64(r.g, f, e->sc[m], e->pc[m], rk, nullptr,
                                                             st, launches);
             if (err != cudaSuccess)

@@ -57,6 +57,7 @@ struct PhysConst {
     double K;             /* K_heatcond */
     int upwind;           /* AC_upwind: the LUPWD terms (selects the kernel variant) */
     int debug_skip_load;  /* acDeviceDebugSkipPlaneLoad: the fault-path test of the tiled kernels */
+    int cfl_sum;          /* AC_additive_timestep: substep 2 also forms the additive CFL sum */
     /* helical forcing of this launch (substep 2 only; forcing = 0 otherwise):
      * u += scale (re cos(a + phase) - im sin(a + phase)), a = sum_d f_k[d] idx_d
      * with idx the interior cell index (mhdsolver.ac:286-331) */
@@ -175,6 +176,7 @@ struct device_s {
     double* adj_pgrad;   /* 2 values: d/d nu, d/d eta */
     double* bfield;      /* AC_lbfield: B = curl A, 3 arrays of mx*my*mz doubles */
     double* adj_tape;    /* substep input states of a recomputed segment, 8 fields each */
+    double* adj_state;   /* FP32 compensated: the joined in-buffers of a per-substep adjoint */
     int adj_tape_states; /* states the tape holds */
     /* graphs of acDeviceAdjointTapeForward, one per in-block, each kept for
      * the next call with the same steps, dt and stream */
@@ -254,10 +256,17 @@ cudaError_t ac_launch_reduce(const Geom& g, const void* const* fields, const flo
 int ac_reduce_blocks(const Geom& g);
 
 /* Tiled substep kernels (solve_tiled.cu): the leading-plane kernel (in-plane
- * derivatives of plane z+3 kept in tensor memory until plane z is solved;
- * the default) and the per-plane tap kernel.  Meshes with the upwinding
- * terms always take the per-plane tap kernel. */
-enum { AC_SOLVE_TILED_LEAD = 1, AC_SOLVE_TILED_TAPS = 2 };
+ * derivatives of plane z+3 kept in tensor memory until plane z is solved) and
+ * the per-plane tap kernel.  AUTO takes the leading-plane kernel for z chunks
+ * of 32 planes and more; _ALT is the leading-plane kernel with the group
+ * exchange through shared memory instead of tensor memory.  Meshes with the
+ * upwinding terms always take the per-plane tap kernel. */
+enum {
+    AC_SOLVE_TILED_AUTO     = 1,
+    AC_SOLVE_TILED_TAPS     = 2,
+    AC_SOLVE_TILED_LEAD     = 3,
+    AC_SOLVE_TILED_LEAD_ALT = 4
+};
 bool ac_tiled_supported(const Geom& g, const int precision);
 bool ac_make_tensor_map(void* map_out, void* base, const Geom& g, const int precision);
 cudaError_t ac_solve_tiled_init(const int precision);

@@ -360,17 +360,33 @@ rk_update_comp(const float h, const float l, const float ph, const float pl, con
 }
 
 /* Per-cell quantities of calc_timestep (acc-runtime/samples/mhd_modular/mhdsolver.ac:551-583):
- * |u|, the Alfven speed sqrt(|B|^2 / rho) and |u| + sqrt(cs_sound^2 + vA^2), folded into
- * running maxima m[3]. */
+ * |u| and the Alfven speed sqrt(|B|^2 / rho) for the maximum form, and, with
+ * `with_sum` (the additive form, AC_additive_timestep), |u| + sqrt(cs_sound^2 + vA^2),
+ * folded into running maxima m[3]; the reference evaluates only the form its
+ * AC_additive_timestep selects.  m[0] and m[1] hold the maxima of the squares
+ * (|u|^2, vA^2): sqrt is correctly rounded and monotone, so cfl_commit's sqrt
+ * of the maximum is the maximum of the square roots, bit for bit.  In FP64 the
+ * sum is formed only where a single-precision estimate of it reaches within
+ * 1e-5 of the running maximum (the estimate's error is below 3e-7 relative), so
+ * the result is the same as evaluating it at every cell. */
 template <typename T>
 __device__ __forceinline__ void
-cfl_accumulate(const T u2, const T b2, const T inv_rho, const T cs2_sound, T m[3])
+cfl_accumulate(const T u2, const T b2, const T inv_rho, const T cs2_sound, T m[3],
+               const bool with_sum = true)
 {
-    const T va2  = b2 * inv_rho;
-    const T umag = sqrt(u2);
-    m[0]         = fmax(m[0], umag);
-    m[1]         = fmax(m[1], sqrt(va2));
-    m[2]         = fmax(m[2], umag + sqrt(cs2_sound + va2));
+    const T va2 = b2 * inv_rho;
+    m[0]        = fmax(m[0], u2);
+    m[1]        = fmax(m[1], va2);
+    if (!with_sum)
+        return;
+    if constexpr (sizeof(T) == 8) {
+        const float est = __fsqrt_rn((float)u2) + __fsqrt_rn((float)(cs2_sound + va2));
+        if (est >= (float)m[2] * 0.99999f)
+            m[2] = fmax(m[2], sqrt(u2) + sqrt(cs2_sound + va2));
+    }
+    else {
+        m[2] = fmax(m[2], sqrt(u2) + sqrt(cs2_sound + va2));
+    }
 }
 
 /* Block-wide max of m[3] across all threads, then one atomicMax per value on
@@ -384,6 +400,8 @@ cfl_commit(T m[3], T* red, unsigned long long* cfl)
     const int nthreads = blockDim.x * blockDim.y;
     const int tid      = threadIdx.y * blockDim.x + threadIdx.x;
     const int warp     = tid >> 5;
+    m[0]               = sqrt(m[0]); /* cfl_accumulate keeps the squares of these two */
+    m[1]               = sqrt(m[1]);
 #pragma unroll
     for (int i = 0; i < 3; ++i)
 #pragma unroll

@@ -95,7 +95,8 @@ plain_cell(const Geom& g, const F& f, const StencilT<T>& sc, const PhysConst& pc
     if (cfl) {
         const T Bx = A.g[2][1] - A.g[1][2], By = A.g[0][2] - A.g[2][0], Bz = A.g[1][0] - A.g[0][1];
         cfl_accumulate(U.v[0] * U.v[0] + U.v[1] * U.v[1] + U.v[2] * U.v[2],
-                       Bx * Bx + By * By + Bz * Bz, ac_exp(-L.v), p.cs2_sound, cm);
+                       Bx * Bx + By * By + Bz * Bz, ac_exp(-L.v), p.cs2_sound, cm,
+                       pc.cfl_sum != 0);
     }
 
     const T val[AC_NF] = {L.v, U.v[0], U.v[1], U.v[2], A.v[0], A.v[1], A.v[2], S.v};

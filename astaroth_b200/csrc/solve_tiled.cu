@@ -419,7 +419,7 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
                     const T* B = &mx.a[M2H_B];
                     cfl_accumulate(u[0] * u[0] + u[1] * u[1] + u[2] * u[2],
                                    B[0] * B[0] + B[1] * B[1] + B[2] * B[2], hx.a[H2M_INV_RHO],
-                                   p.cs2_sound, cm);
+                                   p.cs2_sound, cm, pc.cfl_sum != 0);
                 }
                 val[0] = vd.v[0];
                 val[1] = vd.v[1];
@@ -508,79 +508,149 @@ struct LeadTm<float> {
 };
 
 /* record of one plane and warp group (index: value) */
-constexpr int NREC      = 19;
+constexpr int NREC      = 18;
 constexpr int REC_SD1X  = 0;  /* scalar d/dx */
 constexpr int REC_SD1Y  = 1;  /* scalar d/dy */
 constexpr int REC_SLAP  = 2;  /* scalar second-derivative side sums, x + y */
 constexpr int REC_V     = 3;  /* + 4c + {0: d/dx, 1: d/dy, 2: x sides, 3: y sides} of component c */
 constexpr int REC_DXY0  = 15; /* D_xy of component 0 (enters grad div, y) */
-constexpr int REC_E     = 16; /* group 0 only: exp(gamma s/cp + (gamma-1)(lnrho - lnrho0)) */
-constexpr int REC_IRHO  = 17; /* group 0 only: exp(-lnrho) */
-constexpr int REC_DXY1  = 18; /* D_xy of component 1 (enters grad div, x) */
+constexpr int REC_EXP   = 16; /* group 0: exp(-lnrho); group 1: exp(gamma s/cp + (gamma-1)(lnrho - lnrho0)) */
+constexpr int REC_DXY1  = 17; /* D_xy of component 1 (enters grad div, x) */
 
-template <typename T>
+/* Shared memory of the leading-plane kernel: the plane ring, the group
+ * exchange through shared memory in two buffers (alternate planes; none when
+ * the exchange goes through TMEM), 256 B for the CFL commit, the ring's
+ * mbarriers and the TMEM base address. */
+constexpr int XROWS = 15; /* exchange rows: 6 hydro -> magnetic, 9 magnetic -> hydro */
+template <typename T, bool XT>
+struct LeadSmem {
+    static constexpr size_t RING_B = (size_t)RING * Layout<T>::SLOT_BYTES;
+    static constexpr size_t XCH_B  = XT ? 0 : 2 * (size_t)XROWS * NCELL * sizeof(T);
+    static constexpr size_t RED_B  = 256;
+    static constexpr size_t BAR_OFF = RING_B + XCH_B + RED_B;
+    static constexpr size_t BYTES  = BAR_OFF + RING * sizeof(uint64_t) + 16;
+};
+template <typename T, bool XT>
 constexpr size_t lead_smem_bytes()
 {
-    return Layout<T>::SMEM_BYTES + 16; /* + the TMEM base address */
+    return LeadSmem<T, XT>::BYTES;
 }
 
-/* Column offsets of a record's three parts: A = entries 0..15, B = 16..17 (the
- * two exponentials), C = entry 18; as 32-bit words (two per double). */
+/* Column offsets of a record's three parts: A = entries 0..15, B = entry 16
+ * (the group's exponential, which the other group reads too), C = entry 17; as
+ * 32-bit words (two per double). */
 template <typename T>
 struct RecCols {
     static constexpr int WE = (int)sizeof(T) / 4; /* words per entry */
     static constexpr int B  = 16 * WE;
-    static constexpr int C  = 18 * WE;
+    static constexpr int C  = 17 * WE;
 };
 
-template <typename T, bool WITH_B>
+template <typename T>
 __device__ __forceinline__ void
 rec_store(const uint32_t a, const tmem::Words<T, NREC>& r)
 {
     typedef RecCols<T> RC;
     if constexpr (sizeof(T) == 8) {
         tmem::st32(a, r.w);
-        if constexpr (WITH_B)
-            tmem::st4(a + RC::B, r.w + RC::B);
-        tmem::st2(a + RC::C, r.w + RC::C);
+        tmem::st4(a + RC::B, r.w + RC::B); /* entries 16 and 17 */
     }
     else {
         tmem::st16(a, r.w);
-        if constexpr (WITH_B)
-            tmem::st2(a + RC::B, r.w + RC::B);
-        tmem::st1(a + RC::C, r.w[RC::C]);
+        tmem::st2(a + RC::B, r.w + RC::B);
     }
 }
 
-template <typename T, bool WITH_B>
+template <typename T>
 __device__ __forceinline__ void
 rec_load(const uint32_t a, tmem::Words<T, NREC>& r)
 {
     typedef RecCols<T> RC;
     if constexpr (sizeof(T) == 8) {
         tmem::ld32(a, r.w);
-        if constexpr (WITH_B)
-            tmem::ld4(a + RC::B, r.w + RC::B);
-        tmem::ld2(a + RC::C, r.w + RC::C);
+        tmem::ld4(a + RC::B, r.w + RC::B);
     }
     else {
         tmem::ld16(a, r.w);
-        if constexpr (WITH_B)
-            tmem::ld2(a + RC::B, r.w + RC::B);
-        tmem::ld1(a + RC::C, r.w + RC::C);
+        tmem::ld2(a + RC::B, r.w + RC::B);
     }
 }
 
-/* part B alone (the exponentials of another group's record) */
+/* entry 16 (the exponential) of another group's record */
 template <typename T>
 __device__ __forceinline__ void
-rec_load_b(const uint32_t a, tmem::Words<T, NREC>& r)
+rec_load_exp(const uint32_t a, tmem::Words<T, 1>& r)
 {
     typedef RecCols<T> RC;
     if constexpr (sizeof(T) == 8)
-        tmem::ld4(a + RC::B, r.w + RC::B);
+        tmem::ld2(a + RC::B, r.w);
     else
-        tmem::ld2(a + RC::B, r.w + RC::B);
+        tmem::ld1(a + RC::B, r.w);
+}
+
+/* The exchange between the warp groups through tensor memory (the default):
+ * group 0's six values (grad lnrho, lap lnrho, S:S, div u) and group
+ * 1's nine (grad s, j, B) in the unused columns of record slot 0 or 1 (by
+ * plane parity), from column XCol of each group's space (the records take 36
+ * of a slot's 64 columns in FP64 and 18 of 32 in FP32). */
+template <typename T>
+struct XCol {
+    static constexpr uint32_t value = sizeof(T) == 8 ? 40 : 20;
+};
+
+template <typename T>
+__device__ __forceinline__ void
+xt_store6(const uint32_t a, const tmem::Words<T, 6>& v)
+{
+    if constexpr (sizeof(T) == 8) {
+        tmem::st8(a, v.w);
+        tmem::st4(a + 8, v.w + 8);
+    }
+    else {
+        tmem::st4(a, v.w);
+        tmem::st2(a + 4, v.w + 4);
+    }
+}
+template <typename T>
+__device__ __forceinline__ void
+xt_load6(const uint32_t a, tmem::Words<T, 6>& v)
+{
+    if constexpr (sizeof(T) == 8) {
+        tmem::ld8(a, v.w);
+        tmem::ld4(a + 8, v.w + 8);
+    }
+    else {
+        tmem::ld4(a, v.w);
+        tmem::ld2(a + 4, v.w + 4);
+    }
+}
+template <typename T>
+__device__ __forceinline__ void
+xt_store9(const uint32_t a, const tmem::Words<T, 9>& v)
+{
+    if constexpr (sizeof(T) == 8) {
+        tmem::st8(a, v.w);
+        tmem::st8(a + 8, v.w + 8);
+        tmem::st2(a + 16, v.w + 16);
+    }
+    else {
+        tmem::st8(a, v.w);
+        tmem::st1(a + 8, v.w[8]);
+    }
+}
+template <typename T>
+__device__ __forceinline__ void
+xt_load9(const uint32_t a, tmem::Words<T, 9>& v)
+{
+    if constexpr (sizeof(T) == 8) {
+        tmem::ld8(a, v.w);
+        tmem::ld8(a + 8, v.w + 8);
+        tmem::ld2(a + 16, v.w + 16);
+    }
+    else {
+        tmem::ld8(a, v.w);
+        tmem::ld1(a + 8, v.w + 8);
+    }
 }
 
 /* differences and sums of one field along x (or y) at this cell of a plane:
@@ -650,11 +720,12 @@ struct LeadPhase {
 /* The whole chunk for the threads of one warp group (GROUP 0: lnrho and uu,
  * GROUP 1: aa and entropy).  Both groups take the same barriers in the same
  * order. */
-template <typename T, bool COMP, int GROUP>
+template <typename T, bool COMP, int GROUP, bool XT>
 __device__ __forceinline__ void
 lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const StencilT<T>& sc,
-           const PhysT<T>& p, const RkCoef& rk, int* err, unsigned long long* cfl, T* smem, T* xh,
-           T* xm, uint64_t* bars, const uint32_t tcol, const int zchunk, const bool skip_last)
+           const PhysT<T>& p, const RkCoef& rk, int* err, unsigned long long* cfl, T* smem, T* xch,
+           T* red, uint64_t* bars, const uint32_t tcol, const int zchunk, const bool skip_last,
+           const bool cfl_sum)
 {
     const long long wlim = skip_last ? kDebugWaitLimit : kWaitLimit;
     typedef Layout<T> L;
@@ -729,10 +800,11 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
 
         /* record of plane z, stored three steps ago */
         tmem::Words<T, NREC> rz;
+        tmem::Words<T, 1> ro; /* the other group's exponential of plane z */
         if constexpr (SOLVE) {
-            rec_load<T, GROUP == 0>(tcol + (uint32_t)(z & 3) * TM::SLOT, rz);
-            if constexpr (GROUP == 1) /* the exponentials from group 0's record of plane z */
-                rec_load_b<T>(tcol - TM::GROUP + (uint32_t)(z & 3) * TM::SLOT, rz);
+            rec_load<T>(tcol + (uint32_t)(z & 3) * TM::SLOT, rz);
+            const uint32_t other = GROUP == 0 ? tcol + TM::GROUP : tcol - TM::GROUP;
+            rec_load_exp<T>(other + (uint32_t)(z & 3) * TM::SLOT, ro);
         }
 
         /* ---- plane lp: in-plane differences, record, running mixed sums ---- */
@@ -777,16 +849,18 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
             }
             r.set(REC_DXY0, dxy_at(pl + Q0 * L::PLANE, sc.mix[0]));
             r.set(REC_DXY1, dxy_at(pl + (Q0 + 1) * L::PLANE, sc.mix[0]));
+            /* the RHS's two exponentials (the expressions of hydro_prepare), one
+             * per group, off the solve's critical path; each group reads the
+             * other's from the shared lane */
             if constexpr (GROUP == 0) {
-                /* the two exponentials of the RHS (the expressions of
-                 * hydro_prepare), for both groups, off the solve's critical path */
-                const T lv  = zq[6];
-                const T sv  = pl[VTXBUF_ENTROPY * L::PLANE];
-                const T arg = p.gamma_inv_cp * sv + p.gamma_m1 * (lv - p.lnrho0);
-                r.set(REC_E, ac_exp(arg));
-                r.set(REC_IRHO, ac_exp(-lv));
+                r.set(REC_EXP, ac_exp(-zq[6]));
             }
-            rec_store<T, GROUP == 0>(tcol + (uint32_t)(lp & 3) * TM::SLOT, r);
+            else {
+                const T lv  = pl[VTXBUF_LNRHO * L::PLANE];
+                const T arg = p.gamma_inv_cp * zq[6] + p.gamma_m1 * (lv - p.lnrho0);
+                r.set(REC_EXP, ac_exp(arg));
+            }
+            rec_store<T>(tcol + (uint32_t)(lp & 3) * TM::SLOT, r);
         }
         else {
             /* halo planes only feed the mixed sums */
@@ -838,6 +912,10 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
                 sz2        = fma(d[3], zq[6] + zq[0], b);
             }
             tmem::wait_ld_tied<NW>(rz.w);
+            tmem::wait_ld_tied<tmem::Words<T, 1>::W>(ro.w);
+            /* E = exp(gamma s/cp + (gamma-1)(lnrho - lnrho0)) and 1/rho = exp(-lnrho) */
+            const T e_cs  = GROUP == 0 ? ro.get(0) : rz.get(REC_EXP);
+            const T e_irh = GROUP == 0 ? rz.get(REC_EXP) : ro.get(0);
             const T csum = sc.d2[0][0] + sc.d2[1][0] + sc.d2[2][0];
             sd.v         = zq[3];
             sd.g[0]      = rz.get(REC_SD1X);
@@ -861,30 +939,96 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
             /* group 0 sends grad lnrho, lap lnrho, S:S and div u; group 1 takes u
              * from the ring and the exponentials from group 0's record */
             constexpr int k0 = H2M_GL, k1 = H2M_DIVU + 1;
+            /* the exchange alternates between two buffers by plane parity, so the
+             * exchange barrier of the next plane also guards its reuse: in TMEM
+             * the unused columns of record slots 0 and 1 of each group, in shared
+             * memory two blocks of 15 rows */
+            const uint32_t xslot  = (uint32_t)(lp & 1) * TM::SLOT + XCol<T>::value;
+            const uint32_t xmine  = tcol + xslot;
+            const uint32_t xother = GROUP == 0 ? tcol + TM::GROUP + xslot : tcol - TM::GROUP + xslot;
+            T* xh = xch + (size_t)(lp & 1) * XROWS * NCELL; /* rows 0..5 */
+            T* xm = xh + (size_t)(k1 - k0) * NCELL;         /* rows 6..14 */
             if constexpr (GROUP == 0) {
-                hydro_prepare_exp(sd, vd, rz.get(REC_E), rz.get(REC_IRHO), hx, st);
+                hydro_prepare_exp(sd, vd, e_cs, e_irh, hx, st);
+                if constexpr (XT) {
+                    tmem::Words<T, 6> xw;
 #pragma unroll
-                for (int k = k0; k < k1; ++k)
-                    xh[k * NCELL + cell] = hx.a[k];
+                    for (int k = k0; k < k1; ++k)
+                        xw.set(k - k0, hx.a[k]);
+                    __syncwarp();
+                    xt_store6<T>(xmine, xw);
+                }
+                else {
+#pragma unroll
+                    for (int k = k0; k < k1; ++k)
+                        xh[(k - k0) * NCELL + cell] = hx.a[k];
+                }
             }
             else {
                 mag_prepare(sd, vd, p, mx);
-                hx.a[H2M_E]       = rz.get(REC_E);
-                hx.a[H2M_INV_RHO] = rz.get(REC_IRHO);
+                hx.a[H2M_E]       = e_cs;
+                hx.a[H2M_INV_RHO] = e_irh;
                 hx.a[H2M_U + 0]   = t(VTXBUF_UUX, 0, 0, 0);
                 hx.a[H2M_U + 1]   = t(VTXBUF_UUY, 0, 0, 0);
                 hx.a[H2M_U + 2]   = t(VTXBUF_UUZ, 0, 0, 0);
+                if constexpr (XT) {
+                    tmem::Words<T, 9> xw;
 #pragma unroll
-                for (int k = 0; k < AC_M2H_COUNT; ++k)
-                    xm[k * NCELL + cell] = mx.a[k];
+                    for (int k = 0; k < AC_M2H_COUNT; ++k)
+                        xw.set(k, mx.a[k]);
+                    __syncwarp();
+                    xt_store9<T>(xmine, xw);
+                }
+                else {
+#pragma unroll
+                    for (int k = 0; k < AC_M2H_COUNT; ++k)
+                        xm[k * NCELL + cell] = mx.a[k];
+                }
             }
-            __syncthreads(); /* exchange records written */
+            /* The step's one block barrier: the exchange values are written; every
+             * thread is done with plane lp - 6 (its z taps were read above), whose
+             * ring slot takes plane lp + 2 next; the records stored in this step
+             * and earlier are visible to the other group after it. */
+            tmem::wait_st();
+            tmem::fence_before_sync();
+            __syncthreads();
+            tmem::fence_after_sync();
+            {
+                const int next = lp + 2; /* = lp - 6 + RING */
+                if (tid == 0 && next <= plast && !(skip_last && next == plast)) {
+                    const int sl = (next - pfirst) & (RING - 1);
+                    mbar_arrive_expect_tx(&bars[sl], L::SLOT_BYTES);
+                    tma_load_plane(smem + (size_t)sl * L::SLOT, tmap, &bars[sl], x0, y0,
+                                   next + NGHOST);
+                }
+            }
+            if constexpr (XT) {
+                __syncwarp();
+                if constexpr (GROUP == 0) {
+                    tmem::Words<T, 9> xw;
+                    xt_load9<T>(xother, xw);
+                    tmem::wait_ld_tied<tmem::Words<T, 9>::W>(xw.w);
+#pragma unroll
+                    for (int k = 0; k < AC_M2H_COUNT; ++k)
+                        mx.a[k] = xw.get(k);
+                }
+                else {
+                    tmem::Words<T, 6> xw;
+                    xt_load6<T>(xother, xw);
+                    tmem::wait_ld_tied<tmem::Words<T, 6>::W>(xw.w);
+#pragma unroll
+                    for (int k = k0; k < k1; ++k)
+                        hx.a[k] = xw.get(k - k0);
+                }
+            }
             if (active) {
                 T rr[4], val[4];
                 if constexpr (GROUP == 0) {
+                    if constexpr (!XT) {
 #pragma unroll
-                    for (int k = 0; k < AC_M2H_COUNT; ++k)
-                        mx.a[k] = xm[k * NCELL + cell];
+                        for (int k = 0; k < AC_M2H_COUNT; ++k)
+                            mx.a[k] = xm[k * NCELL + cell];
+                    }
                     hydro_rates(sd, vd, st, hx, mx, p, rr);
                     val[0] = sd.v;
                     val[1] = vd.v[0];
@@ -892,16 +1036,18 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
                     val[3] = vd.v[2];
                 }
                 else {
+                    if constexpr (!XT) {
 #pragma unroll
-                    for (int k = k0; k < k1; ++k)
-                        hx.a[k] = xh[k * NCELL + cell];
+                        for (int k = k0; k < k1; ++k)
+                            hx.a[k] = xh[(k - k0) * NCELL + cell];
+                    }
                     mag_rates(sd, vd, mx, hx, p, rr);
                     if (cfl) {
                         const T* u = &hx.a[H2M_U];
                         const T* B = &mx.a[M2H_B];
                         cfl_accumulate(u[0] * u[0] + u[1] * u[1] + u[2] * u[2],
                                        B[0] * B[0] + B[1] * B[1] + B[2] * B[2],
-                                       hx.a[H2M_INV_RHO], p.cs2_sound, cm);
+                                       hx.a[H2M_INV_RHO], p.cs2_sound, cm, cfl_sum);
                     }
                     val[0] = vd.v[0];
                     val[1] = vd.v[1];
@@ -935,19 +1081,14 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
                 acc[a][j] = acc[a][j + 1];
             acc[a][6] = 0;
         }
-        /* every thread is done with plane lp - 6 and the exchange; the records
-         * stored in this step are visible to the other group after the barrier */
-        tmem::wait_st();
-        tmem::fence_before_sync();
-        __syncthreads();
-        tmem::fence_after_sync();
-        if constexpr (SOLVE) {
-            const int next = lp + 2; /* = lp - 6 + RING, in the slot of plane lp - 6 */
-            if (tid == 0 && next <= plast && !(skip_last && next == plast)) {
-                const int s = (next - pfirst) & (RING - 1);
-                mbar_arrive_expect_tx(&bars[s], L::SLOT_BYTES);
-                tma_load_plane(smem + (size_t)s * L::SLOT, tmap, &bars[s], x0, y0, next + NGHOST);
-            }
+        if constexpr (!SOLVE) {
+            /* a step without a solve: the records stored are visible to the other
+             * group after this barrier (no ring slot is freed before the first
+             * solve) */
+            tmem::wait_st();
+            tmem::fence_before_sync();
+            __syncthreads();
+            tmem::fence_after_sync();
         }
     };
 
@@ -965,13 +1106,15 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
     for (; lp <= plast; ++lp)
         step(LeadPhase<false, true>{}, lp);
 
-    if (cfl)
-        cfl_commit(cm, xh, cfl);
+    if (cfl) {
+        __syncthreads(); /* every thread's last exchange reads are done */
+        cfl_commit(cm, red, cfl);
+    }
     if (!ok)
         atomicExch(err, 1);
 }
 
-template <typename T, bool COMP>
+template <typename T, bool COMP, bool XT>
 __global__ void __launch_bounds__(2 * TX * TY, Tile<T>::MINB)
 solve_lead_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const FieldsT<T> f,
                   const StencilT<T> sc, const PhysConst pc, const RkCoef rk, int* err,
@@ -980,11 +1123,11 @@ solve_lead_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const 
     typedef Layout<T> L;
     typedef LeadTm<T> TM;
     extern __shared__ __align__(128) unsigned char smem_raw[];
+    typedef LeadSmem<T, XT> LS;
     T* smem         = reinterpret_cast<T*>(smem_raw);
-    T* xh           = smem + (size_t)RING * L::SLOT;
-    T* xm           = xh + (size_t)AC_H2M_COUNT * NCELL;
-    uint64_t* bars  = reinterpret_cast<uint64_t*>(smem_raw + (size_t)RING * L::SLOT_BYTES +
-                                                 (size_t)XCHG * sizeof(T));
+    T* xch          = reinterpret_cast<T*>(smem_raw + LS::RING_B);
+    T* red          = reinterpret_cast<T*>(smem_raw + LS::RING_B + LS::XCH_B);
+    uint64_t* bars  = reinterpret_cast<uint64_t*>(smem_raw + LS::BAR_OFF);
     uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + RING);
     const int warp  = threadIdx.y; /* blockDim.x == 32 */
     const int group = threadIdx.y / TY;
@@ -1024,11 +1167,11 @@ solve_lead_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const 
     const PhysT<T> p        = phys_cast<T>(pc);
     const StencilT<T> scv   = sc;
     if (group == 0)
-        lead_group<T, COMP, 0>(&tmap, g, f, scv, p, rk, err, cfl, smem, xh, xm, bars, tcol,
-                               zchunk, skip_last);
+        lead_group<T, COMP, 0, XT>(&tmap, g, f, scv, p, rk, err, cfl, smem, xch, red, bars, tcol,
+                               zchunk, skip_last, pc.cfl_sum != 0);
     else
-        lead_group<T, COMP, 1>(&tmap, g, f, scv, p, rk, err, cfl, smem, xh, xm, bars, tcol,
-                               zchunk, skip_last);
+        lead_group<T, COMP, 1, XT>(&tmap, g, f, scv, p, rk, err, cfl, smem, xch, red, bars, tcol,
+                               zchunk, skip_last, pc.cfl_sum != 0);
     /* no copy into this block's shared memory is left in flight */
     if (tid == 0)
         drain_ring(bars, RING, [&](const int sl) { return loads_into(sl, pfirst, plast, skip_last); });
@@ -1086,12 +1229,28 @@ launch_tiled(const Geom& g, const void* tmap_in, const FieldsT<T>& f, const Sten
     const dim3 tpb(TX, 2 * TY, 1);
     const int zc = zchunk_for(g);
     const dim3 bpg((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + zc - 1) / zc);
+    /* The leading-plane kernel forms stage 1 for the 6 halo planes of every z
+     * chunk too; on short chunks (small meshes) that overhead loses to the
+     * per-plane tap kernel, so the automatic choice takes it from 32 planes. */
+    const int k = kernel == AC_SOLVE_TILED_AUTO
+                      ? (zc >= 32 ? AC_SOLVE_TILED_LEAD : AC_SOLVE_TILED_TAPS)
+                      : kernel;
     if (pc.upwind)
         solve_tiled_kernel<T, COMP, true><<<bpg, tpb, Layout<T>::SMEM_BYTES, stream>>>(
             *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err, cfl, zc);
-    else if (kernel == AC_SOLVE_TILED_LEAD)
-        solve_lead_kernel<T, COMP><<<bpg, tpb, lead_smem_bytes<T>(), stream>>>(
-            *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err, cfl, zc);
+    else if (k == AC_SOLVE_TILED_LEAD || k == AC_SOLVE_TILED_LEAD_ALT) {
+        /* the exchange between the warp groups goes through tensor memory; _ALT
+         * takes shared memory instead (measured at 512^3: 33.6 against 34.2 ms
+         * per FP64 step, and in FP32 the second shared-memory buffer costs the
+         * second block per SM: 24.9 against 27.5 ms) */
+        const bool xt = k != AC_SOLVE_TILED_LEAD_ALT;
+        if (xt)
+            solve_lead_kernel<T, COMP, true><<<bpg, tpb, lead_smem_bytes<T, true>(), stream>>>(
+                *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err, cfl, zc);
+        else
+            solve_lead_kernel<T, COMP, false><<<bpg, tpb, lead_smem_bytes<T, false>(), stream>>>(
+                *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err, cfl, zc);
+    }
     else
         solve_tiled_kernel<T, COMP, false><<<bpg, tpb, Layout<T>::SMEM_BYTES, stream>>>(
             *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err, cfl, zc);
@@ -1168,8 +1327,11 @@ ac_solve_tiled_init(const int precision)
             (e = set_smem<double>((const void*)solve_tiled_kernel<double, false, true>,
                                   L::SMEM_BYTES)) != cudaSuccess)
             return e;
-        return set_smem<double>((const void*)solve_lead_kernel<double, false>,
-                                lead_smem_bytes<double>());
+        if ((e = set_smem<double>((const void*)solve_lead_kernel<double, false, true>,
+                                  lead_smem_bytes<double, true>())) != cudaSuccess)
+            return e;
+        return set_smem<double>((const void*)solve_lead_kernel<double, false, false>,
+                                lead_smem_bytes<double, false>());
     }
     typedef Layout<float> L;
     if ((e = set_smem<float>((const void*)solve_tiled_kernel<float, true, false>,
@@ -1177,7 +1339,11 @@ ac_solve_tiled_init(const int precision)
         (e = set_smem<float>((const void*)solve_tiled_kernel<float, true, true>, L::SMEM_BYTES)) !=
             cudaSuccess)
         return e;
-    return set_smem<float>((const void*)solve_lead_kernel<float, true>, lead_smem_bytes<float>());
+    if ((e = set_smem<float>((const void*)solve_lead_kernel<float, true, true>,
+                             lead_smem_bytes<float, true>())) != cudaSuccess)
+        return e;
+    return set_smem<float>((const void*)solve_lead_kernel<float, true, false>,
+                           lead_smem_bytes<float, false>());
 }
 
 cudaError_t

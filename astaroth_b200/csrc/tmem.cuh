@@ -100,6 +100,14 @@ st4(const uint32_t a, const uint32_t* v)
                  "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]));
 }
 __device__ __forceinline__ void
+st8(const uint32_t a, const uint32_t* v)
+{
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(
+                     a),
+                 "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]),
+                 "r"(v[7]));
+}
+__device__ __forceinline__ void
 st16(const uint32_t a, const uint32_t* v)
 {
     asm volatile("tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], "
@@ -142,6 +150,14 @@ ld4(const uint32_t a, uint32_t* v)
 {
     asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
                  : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3])
+                 : "r"(a));
+}
+__device__ __forceinline__ void
+ld8(const uint32_t a, uint32_t* v)
+{
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]),
+                   "=r"(v[6]), "=r"(v[7])
                  : "r"(a));
 }
 __device__ __forceinline__ void

@@ -22,9 +22,10 @@ aa ~ N(0, 1e-4^2)), nu = eta = 5e-3, cs = 1, gamma = 5/3, dt = 1e-3.
               against the measured HBM copy bandwidth.
 * cpu_baseline  the reference's own host model (oracle/_ref) on the host cores,
               a bounded sample (one RK3 step at 128^3), rank 0 at N=1.
-* ensemble    64 independent FP32-compensated members of sizes {32,48,64,96}^3
-              in one persistent launch per substep, graph-captured step, tiles
-              from the autotuner; against sequential per-member plain launches.
+* ensemble    64 independent FP32-compensated members of sizes {32,48,64,96}^3,
+              graph-captured step in the autotuner's mode (persistent work list or
+              per-member tiled launches as graph branches); against the members
+              advanced one by one, a Device per member through acDeviceIntegrateStep.
 * fp32comp    the same workload with FP32 fields and a compensated FP32 hi/lo RK3
               state (AC_precision = 1): cell-updates/s, speed-up over FP64, and
               the per-field relative L-inf against the FP64 path after 100 steps
@@ -552,8 +553,12 @@ def ensemble_leg(args, torch, rank, world):
     for _ in range(args.warmup):
         e.integrate_step_sequential()
     l1 = e.launch_count()
-    ms_seq = timed(e.integrate_step_sequential, k)
-    launches_seq = (e.launch_count() - l1) // k
+    ms_plain = timed(e.integrate_step_sequential, k)
+    launches_plain = (e.launch_count() - l1) // k
+    # the one-by-one arm: one single-mesh Device per member, each stepped with
+    # acDeviceIntegrateStep (its default tiled kernel, its own streams)
+    ms_seq, launches_seq = device_loop_ms(torch, [members[m] for m in mine], k, args.warmup)
+    ms_seq = adist.max_over_ranks(ms_seq)
     # both step modes with the tuned work-list tiles, for the record
     modes = {}
     for mode in (0, 1):
@@ -574,8 +579,15 @@ def ensemble_leg(args, torch, rank, world):
             "members": len(members), "cells": total_cells, "value": total_cells / (ms * 1e-3),
             "unit": UNIT, "ms_per_step": ms, "steps": k, "gpu_launches_per_step": launches,
             "sequential": {"value": total_cells / (ms_seq * 1e-3), "ms_per_step": ms_seq,
-                           "gpu_launches_per_step": launches_seq},
-            "speedup_vs_sequential": ms_seq / ms, "tiles": list(tiles),
+                           "gpu_launches_per_step": launches_seq,
+                           "how": "one single-mesh Device per member, acDeviceIntegrateStep "
+                                  "on each in turn (default tiled kernel, the Devices' own "
+                                  "streams); CUDA events joined over all member streams"},
+            "speedup_vs_sequential": ms_seq / ms,
+            "plain_sequential": {"ms_per_step": ms_plain, "gpu_launches_per_step": launches_plain,
+                                 "how": "acEnsembleIntegrateStepSequential: per-member plain "
+                                        "(untiled) launches in one stream"},
+            "tiles": list(tiles),
             "ms_per_step_by_mode": {"persistent": modes.get(0),
                                     "tiled_per_member_graph": modes.get(1)},
             "autotune_solve_ms": tune_ms, "clocks": clk.summary(),
@@ -584,6 +596,45 @@ def ensemble_leg(args, torch, rank, world):
                          "bytes_per_cell_step": BYTES_PER_CELL_STEP["fp32comp"],
                          "note": "whole step incl. halo fills"},
             "scaling": "strong (64 members split across ranks)"}
+
+
+def device_loop_ms(torch, members, k, warmup):
+    """ms per RK3 step of the members advanced one by one: a Device per member,
+    acDeviceIntegrateStep on each in turn.  The Devices run on their own
+    streams; the timing joins them with CUDA events on one stream."""
+    import astaroth_b200 as ab
+    devs = []
+    try:
+        for info, seed in members:
+            d = ab.Device(info, device_id=torch.cuda.current_device())
+            d.load_mesh(ab.seeded_mesh(info, seed))
+            devs.append(d)
+        streams = [torch.cuda.ExternalStream(d.stream_handle(0)) for d in devs]
+        for _ in range(warmup):
+            for d in devs:
+                d.integrate_step(1e-3)
+        torch.cuda.synchronize()
+        main = torch.cuda.current_stream()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        l0 = sum(d.launch_count() for d in devs)
+        e0.record(main)
+        for st in streams:
+            st.wait_event(e0)
+        for _ in range(k):
+            for d in devs:
+                d.integrate_step(1e-3)
+        for st in streams:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            main.wait_event(ev)
+        e1.record(main)
+        e1.synchronize()
+        launches = (sum(d.launch_count() for d in devs) - l0) // k
+        return e0.elapsed_time(e1) / k, launches
+    finally:
+        for d in devs:
+            d.destroy()
 
 
 def ab_cells(info):

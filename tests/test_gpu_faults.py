@@ -30,7 +30,9 @@ def clean_step(info, f, kernel):
 
 
 @pytest.mark.parametrize("precision", [0, 1])
-@pytest.mark.parametrize("kernel", [0, 2])  # the default tiled kernel, the per-plane tap kernel
+# the leading-plane kernel with the group exchange through tensor memory or
+# shared memory, the per-plane tap kernel
+@pytest.mark.parametrize("kernel", [3, 4, 2])
 def test_bounded_wait_gives_up_and_device_recovers(precision, kernel):
     info = ab.make_info((64, 16, 40), precision=precision, **ab.CONFIG_PARAMS)
     f = ab.seeded_mesh(info, 3)

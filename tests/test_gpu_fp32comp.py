@@ -103,9 +103,13 @@ def test_plain_and_tiled_fp32comp_agree(n):
     assert err.max() <= 1e-8, err
     # the default kernel sums the mixed derivatives in another order: agreement
     # to FP32 rounding (2^-24 = 6e-8 relative per operation)
-    b = run(n, 6, 2, precision=1, plain=False)
+    b = run(n, 6, 2, precision=1, kernel=3)
     err = oracle.rel_linf(a, b)
     assert err.max() <= 1e-7, err
+    # the exchange between the warp groups through shared memory instead of
+    # tensor memory: the same bits
+    d = run(n, 6, 2, precision=1, kernel=4)
+    assert np.array_equal(d, b)
 
 
 def test_graph_and_loop_agree_fp32comp():
