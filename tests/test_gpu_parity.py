@@ -181,11 +181,14 @@ def test_large_amplitude_other_params():
     assert err.max() <= TOL_1STEP * 10, err
 
 
-def test_graph_step_equals_loop_bitwise():
-    info = ab.make_info(48, **ab.CONFIG_PARAMS)
+@pytest.mark.parametrize("kernel", [0, 3])
+def test_graph_step_equals_loop_bitwise(kernel):
+    """The graph-captured step equals halo fill + substep + swap three times, with
+    the default kernel choice and with the leading-plane kernel (3)."""
+    info = ab.make_info((64, 40, 48), **ab.CONFIG_PARAMS)
     f = ab.seeded_mesh(info, 4)
-    a = gpu_run(info, f, 1e-3, 3, graph=False)
-    b = gpu_run(info, f, 1e-3, 3, graph=True)
+    a = gpu_run(info, f, 1e-3, 3, graph=False, kernel=kernel)
+    b = gpu_run(info, f, 1e-3, 3, graph=True, kernel=kernel)
     assert np.array_equal(oracle.interior(a), oracle.interior(b))
 
 
