@@ -472,7 +472,7 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
  *   D^k f = f(+k) - f(-k) and sums S^k = f(+k) + f(-k) (k = 1..3) of its
  *   group's fields at its cell, and from them the in-plane first and second
  *   derivatives and the diagonal xy mixed derivatives of plane L.  These 17
- *   values per group (its record) go to tensor memory (TMEM), a 4-plane delay
+ *   values per group (its record) go to tensor memory (TMEM), a 3-slot delay
  *   line in the thread's own lane, and come back when plane L is solved three
  *   planes later (the z stencils need planes up to z + 3 first).
  * * The xz and yz mixed derivatives use the separable form of the diagonal
@@ -483,11 +483,16 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
  *   plane L+k, in seven running sums per mixed term held in registers.  Only
  *   the combinations grad(div) needs are formed: D_xz uz, D_yz uz and
  *   D_xz ux + D_yz uy (and the same for aa).
- * * The z first and second derivatives of the vector components still read the
- *   plane ring at plane z (their own column); the scalar field keeps its z
- *   line in registers.
+ * * The z lines: the scalar field's in registers; the vector components' in a
+ *   TMEM queue of the last seven planes, written when a plane arrives (its
+ *   value at the thread's cell, three values per group) and read back as
+ *   planes z-3 .. z+2 in one load when z is solved.  The queue holds each plane
+ *   twice, at entries e and e + 7 (e = plane mod 7), so that the window is
+ *   always one contiguous run of entries and its register positions are fixed.
+ *   The magnetic group reads u at plane z from the hydro group's queue.
+ * * A plane is read from shared memory only in the step it arrives.
  *
- * Per cell and substep this reads ~200 values from shared memory instead of
+ * Per cell and substep this reads ~155 values from shared memory instead of
  * ~320.  The arithmetic per cell is the same up to association (the mixed
  * derivatives are summed in a different order), so results agree with the
  * other kernels to rounding, not bit for bit.
@@ -498,24 +503,51 @@ template <>
 struct LeadTm<double> {
     static constexpr uint32_t NCOLS = 512; /* 1 block per SM */
     static constexpr uint32_t GROUP = 256; /* columns per warp group */
-    static constexpr uint32_t SLOT  = 64;  /* columns per plane record */
 };
 template <>
 struct LeadTm<float> {
     static constexpr uint32_t NCOLS = 256; /* 2 blocks per SM */
     static constexpr uint32_t GROUP = 128;
-    static constexpr uint32_t SLOT  = 32;
 };
 
 /* record of one plane and warp group (index: value) */
-constexpr int NREC      = 18;
+constexpr int NREC      = 17;
 constexpr int REC_SD1X  = 0;  /* scalar d/dx */
 constexpr int REC_SD1Y  = 1;  /* scalar d/dy */
 constexpr int REC_SLAP  = 2;  /* scalar second-derivative side sums, x + y */
 constexpr int REC_V     = 3;  /* + 4c + {0: d/dx, 1: d/dy, 2: x sides, 3: y sides} of component c */
 constexpr int REC_DXY0  = 15; /* D_xy of component 0 (enters grad div, y) */
-constexpr int REC_EXP   = 16; /* group 0: exp(-lnrho); group 1: exp(gamma s/cp + (gamma-1)(lnrho - lnrho0)) */
-constexpr int REC_DXY1  = 17; /* D_xy of component 1 (enters grad div, x) */
+constexpr int REC_DXY1  = 16; /* D_xy of component 1 (enters grad div, x) */
+
+/* A warp group's TMEM columns (32-bit words; WE per value), in its own lanes:
+ *   records   3 slots (plane mod 3) of NREC values; the record of plane z is
+ *             read back in the step that stores plane z + 3's into the same
+ *             slot, after the read has completed;
+ *   EXP       4 slots (plane mod 4) of the group's exponential (group 0:
+ *             exp(-lnrho), group 1: exp(gamma s/cp + (gamma-1)(lnrho - lnrho0))),
+ *             which the other group reads three planes later;
+ *   XCH       the exchange between the groups, two buffers (plane parity) of up
+ *             to nine values;
+ *   ZQ        the z queue: 14 entries of the three vector components. */
+template <typename T>
+struct LeadCols {
+    static constexpr uint32_t WE    = (uint32_t)sizeof(T) / 4;
+    static constexpr uint32_t REC_W = NREC * WE;
+    static constexpr uint32_t EXP0  = 3 * REC_W;
+    static constexpr uint32_t XCH0  = EXP0 + 4 * WE;
+    static constexpr uint32_t XCH_W = 9 * WE;
+    static constexpr uint32_t ZQ0   = XCH0 + 2 * XCH_W;
+    static constexpr uint32_t ZQ_E  = 3 * WE;
+    static constexpr uint32_t END   = ZQ0 + 14 * ZQ_E;
+    static_assert(END <= LeadTm<T>::GROUP, "TMEM columns of a warp group");
+};
+
+/* queue entry of plane p >= -NGHOST */
+__device__ __forceinline__ uint32_t
+zq_entry(const int p)
+{
+    return (uint32_t)(p + NGHOST) % 7u;
+}
 
 /* Shared memory of the leading-plane kernel: the plane ring, the group
  * exchange through shared memory in two buffers (alternate planes; none when
@@ -536,122 +568,9 @@ constexpr size_t lead_smem_bytes()
     return LeadSmem<T, XT>::BYTES;
 }
 
-/* Column offsets of a record's three parts: A = entries 0..15, B = entry 16
- * (the group's exponential, which the other group reads too), C = entry 17; as
- * 32-bit words (two per double). */
-template <typename T>
-struct RecCols {
-    static constexpr int WE = (int)sizeof(T) / 4; /* words per entry */
-    static constexpr int B  = 16 * WE;
-    static constexpr int C  = 17 * WE;
-};
-
-template <typename T>
-__device__ __forceinline__ void
-rec_store(const uint32_t a, const tmem::Words<T, NREC>& r)
-{
-    typedef RecCols<T> RC;
-    if constexpr (sizeof(T) == 8) {
-        tmem::st32(a, r.w);
-        tmem::st4(a + RC::B, r.w + RC::B); /* entries 16 and 17 */
-    }
-    else {
-        tmem::st16(a, r.w);
-        tmem::st2(a + RC::B, r.w + RC::B);
-    }
-}
-
-template <typename T>
-__device__ __forceinline__ void
-rec_load(const uint32_t a, tmem::Words<T, NREC>& r)
-{
-    typedef RecCols<T> RC;
-    if constexpr (sizeof(T) == 8) {
-        tmem::ld32(a, r.w);
-        tmem::ld4(a + RC::B, r.w + RC::B);
-    }
-    else {
-        tmem::ld16(a, r.w);
-        tmem::ld2(a + RC::B, r.w + RC::B);
-    }
-}
-
-/* entry 16 (the exponential) of another group's record */
-template <typename T>
-__device__ __forceinline__ void
-rec_load_exp(const uint32_t a, tmem::Words<T, 1>& r)
-{
-    typedef RecCols<T> RC;
-    if constexpr (sizeof(T) == 8)
-        tmem::ld2(a + RC::B, r.w);
-    else
-        tmem::ld1(a + RC::B, r.w);
-}
-
 /* The exchange between the warp groups through tensor memory (the default):
- * group 0's six values (grad lnrho, lap lnrho, S:S, div u) and group
- * 1's nine (grad s, j, B) in the unused columns of record slot 0 or 1 (by
- * plane parity), from column XCol of each group's space (the records take 36
- * of a slot's 64 columns in FP64 and 18 of 32 in FP32). */
-template <typename T>
-struct XCol {
-    static constexpr uint32_t value = sizeof(T) == 8 ? 40 : 20;
-};
-
-template <typename T>
-__device__ __forceinline__ void
-xt_store6(const uint32_t a, const tmem::Words<T, 6>& v)
-{
-    if constexpr (sizeof(T) == 8) {
-        tmem::st8(a, v.w);
-        tmem::st4(a + 8, v.w + 8);
-    }
-    else {
-        tmem::st4(a, v.w);
-        tmem::st2(a + 4, v.w + 4);
-    }
-}
-template <typename T>
-__device__ __forceinline__ void
-xt_load6(const uint32_t a, tmem::Words<T, 6>& v)
-{
-    if constexpr (sizeof(T) == 8) {
-        tmem::ld8(a, v.w);
-        tmem::ld4(a + 8, v.w + 8);
-    }
-    else {
-        tmem::ld4(a, v.w);
-        tmem::ld2(a + 4, v.w + 4);
-    }
-}
-template <typename T>
-__device__ __forceinline__ void
-xt_store9(const uint32_t a, const tmem::Words<T, 9>& v)
-{
-    if constexpr (sizeof(T) == 8) {
-        tmem::st8(a, v.w);
-        tmem::st8(a + 8, v.w + 8);
-        tmem::st2(a + 16, v.w + 16);
-    }
-    else {
-        tmem::st8(a, v.w);
-        tmem::st1(a + 8, v.w[8]);
-    }
-}
-template <typename T>
-__device__ __forceinline__ void
-xt_load9(const uint32_t a, tmem::Words<T, 9>& v)
-{
-    if constexpr (sizeof(T) == 8) {
-        tmem::ld8(a, v.w);
-        tmem::ld8(a + 8, v.w + 8);
-        tmem::ld2(a + 16, v.w + 16);
-    }
-    else {
-        tmem::ld8(a, v.w);
-        tmem::ld1(a + 8, v.w + 8);
-    }
-}
+ * group 0's six values (grad lnrho, lap lnrho, S:S, div u) and group 1's nine
+ * (grad s, j, B), each group's in its own XCH columns. */
 
 /* differences and sums of one field along x (or y) at this cell of a plane:
  * p points at the field's value there; step is 1 (x) or the row pitch (y) */
@@ -730,9 +649,11 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
     const long long wlim = skip_last ? kDebugWaitLimit : kWaitLimit;
     typedef Layout<T> L;
     typedef LeadTm<T> TM;
+    typedef LeadCols<T> LC;
     constexpr int QS = GROUP == 0 ? VTXBUF_LNRHO : VTXBUF_ENTROPY;
     constexpr int Q0 = GROUP == 0 ? VTXBUF_UUX : VTXBUF_AX;
-    constexpr int NW = tmem::Words<T, NREC>::W;
+    /* the other group's columns in the same lanes */
+    const uint32_t tother = GROUP == 0 ? tcol + TM::GROUP : tcol - TM::GROUP;
     const int lx     = threadIdx.x;
     const int ly     = threadIdx.y & (TY - 1);
     const int tid    = threadIdx.y * TX + lx;
@@ -798,21 +719,44 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
         waited = lp;
         __syncwarp(); /* tensor-memory accesses below are warp-collective */
 
-        /* record of plane z, stored three steps ago */
+        /* record of plane z, stored three steps ago, and the two groups'
+         * exponentials of plane z */
         tmem::Words<T, NREC> rz;
-        tmem::Words<T, 1> ro; /* the other group's exponential of plane z */
+        tmem::Words<T, 1> eo, ro;
         if constexpr (SOLVE) {
-            rec_load<T>(tcol + (uint32_t)(z & 3) * TM::SLOT, rz);
-            const uint32_t other = GROUP == 0 ? tcol + TM::GROUP : tcol - TM::GROUP;
-            rec_load_exp<T>(other + (uint32_t)(z & 3) * TM::SLOT, ro);
+            rz.load(tcol + ((uint32_t)z % 3u) * LC::REC_W);
+            eo.load(tcol + LC::EXP0 + (uint32_t)(z & 3) * LC::WE);
+            ro.load(tother + LC::EXP0 + (uint32_t)(z & 3) * LC::WE);
         }
 
-        /* ---- plane lp: in-plane differences, record, running mixed sums ---- */
+        /* ---- plane lp: the z lines, then (now or after the barrier) the
+         * in-plane differences, record and running mixed sums ---- */
         const T* pl = smem + (size_t)((lp - pfirst) & (RING - 1)) * L::SLOT + cell_off;
 #pragma unroll
         for (int k = 0; k < 6; ++k)
             zq[k] = zq[k + 1];
         zq[6] = pl[QS * L::PLANE];
+        /* the vector at this cell of plane lp: into the z queue (both copies) */
+        tmem::Words<T, 3> cur;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            cur.set(c, pl[(Q0 + c) * L::PLANE]);
+        {
+            const uint32_t qa = tcol + LC::ZQ0 + zq_entry(lp) * LC::ZQ_E;
+            cur.store(qa);
+            cur.store(qa + 7 * LC::ZQ_E);
+        }
+        /* In a solve step the hydro group forms plane lp's in-plane part after
+         * the exchange barrier, in one basic block with its rates: its prepare
+         * needs neither grad div u nor plane lp's record, so its shared-memory
+         * reads overlap the rates' FP64 work, and on each SM sub-partition the
+         * two groups' warps are in different phases before the barrier.  (The
+         * magnetic group's prepare needs grad div A of plane z, complete only
+         * with plane lp's differences: it keeps the in-plane part first.
+         * Measured at 512^3, FP64: 31.2 against 33.6 ms per step with both
+         * groups in-plane first, 36.1 with both late.) */
+        constexpr bool LATE_NOW = SOLVE && GROUP == 0;
+        auto inplane = [&]() {
         T dvx[3], dvy[3], dzx[3], dzy[3]; /* D_x^k v_x, D_y^k v_y, D_x^k v_z, D_y^k v_z */
         if constexpr (INTERIOR) {
             tmem::Words<T, NREC> r;
@@ -852,15 +796,24 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
             /* the RHS's two exponentials (the expressions of hydro_prepare), one
              * per group, off the solve's critical path; each group reads the
              * other's from the shared lane */
+            tmem::Words<T, 1> ex;
             if constexpr (GROUP == 0) {
-                r.set(REC_EXP, ac_exp(-zq[6]));
+                ex.set(0, ac_exp(-zq[6]));
             }
             else {
                 const T lv  = pl[VTXBUF_LNRHO * L::PLANE];
                 const T arg = p.gamma_inv_cp * zq[6] + p.gamma_m1 * (lv - p.lnrho0);
-                r.set(REC_EXP, ac_exp(arg));
+                ex.set(0, ac_exp(arg));
             }
-            rec_store<T>(tcol + (uint32_t)(lp & 3) * TM::SLOT, r);
+            ex.store(tcol + LC::EXP0 + (uint32_t)(lp & 3) * LC::WE);
+            if constexpr (SOLVE) {
+                /* plane z's record, in the slot plane lp's takes, is in registers */
+                tmem::wait_ld();
+                rz.tie();
+                eo.tie();
+                ro.tie();
+            }
+            r.store(tcol + ((uint32_t)lp % 3u) * LC::REC_W);
         }
         else {
             /* halo planes only feed the mixed sums */
@@ -882,24 +835,19 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
             acc[2][3 - k] += a2;
             acc[2][3 + k] -= a2;
         }
+        };
+        if constexpr (!LATE_NOW)
+            inplane();
 
         /* ---- plane z = lp - 3: the RHS and the RK update ---- */
         if constexpr (SOLVE) {
-            Taps<T> t;
-            t.s = smem;
-#pragma unroll
-            for (int k = 0; k < 7; ++k)
-                t.off[k] = ((z - NGHOST + k - pfirst) & (RING - 1)) * L::SLOT + cell_off;
-            ScalD<T> sd;
-            VecD<T> vd;
-            T s2z[3];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const int q = Q0 + c;
-                vd.v[c]     = t(q, 0, 0, 0);
-                vd.g[c][2]  = d1<2>(t, q, sc.d1[2]);
-                s2z[c]      = d2_sides<2>(t, q, sc.d2[2]);
-            }
+            /* planes z-3 .. z+2 of the vector from the queue (z+3 = lp is cur);
+             * the magnetic group also takes u at plane z from the hydro group's */
+            tmem::Words<T, 18> win;
+            win.load(tcol + LC::ZQ0 + zq_entry(z - NGHOST) * LC::ZQ_E);
+            [[maybe_unused]] tmem::Words<T, 3> uz;
+            if constexpr (GROUP == 1)
+                uz.load(tother + LC::ZQ0 + zq_entry(z) * LC::ZQ_E);
             T sz1, sz2;
             {
                 const T* c = sc.d1[2];
@@ -911,11 +859,34 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
                 b          = fma(d[2], zq[5] + zq[1], b);
                 sz2        = fma(d[3], zq[6] + zq[0], b);
             }
-            tmem::wait_ld_tied<NW>(rz.w);
-            tmem::wait_ld_tied<tmem::Words<T, 1>::W>(ro.w);
+            tmem::wait_ld();
+            rz.tie();
+            eo.tie();
+            ro.tie();
+            win.tie();
+            if constexpr (GROUP == 1)
+                uz.tie();
+            ScalD<T> sd;
+            VecD<T> vd;
+            T s2z[3];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                /* window entry e is plane z - 3 + e */
+                const T m3 = win.get(c), m2 = win.get(3 + c), m1 = win.get(6 + c);
+                const T p1 = win.get(12 + c), p2 = win.get(15 + c), p3 = cur.get(c);
+                const T* c1 = sc.d1[2];
+                const T* c2 = sc.d2[2];
+                vd.v[c]     = win.get(9 + c);
+                T a         = c1[0] * (p1 - m1);
+                a           = fma(c1[1], p2 - m2, a);
+                vd.g[c][2]  = fma(c1[2], p3 - m3, a);
+                T b         = c2[1] * (p1 + m1);
+                b           = fma(c2[2], p2 + m2, b);
+                s2z[c]      = fma(c2[3], p3 + m3, b);
+            }
             /* E = exp(gamma s/cp + (gamma-1)(lnrho - lnrho0)) and 1/rho = exp(-lnrho) */
-            const T e_cs  = GROUP == 0 ? ro.get(0) : rz.get(REC_EXP);
-            const T e_irh = GROUP == 0 ? rz.get(REC_EXP) : ro.get(0);
+            const T e_cs  = GROUP == 0 ? ro.get(0) : eo.get(0);
+            const T e_irh = GROUP == 0 ? eo.get(0) : ro.get(0);
             const T csum = sc.d2[0][0] + sc.d2[1][0] + sc.d2[2][0];
             sd.v         = zq[3];
             sd.g[0]      = rz.get(REC_SD1X);
@@ -929,9 +900,17 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
                 vd.lap[c]  = csum * vd.v[c] + rz.get(REC_V + 4 * c + 2) +
                             rz.get(REC_V + 4 * c + 3) + s2z[c];
             }
-            vd.gd[0] = sc.d2[0][0] * vd.v[0] + rz.get(REC_V + 2) + rz.get(REC_DXY1) + acc[0][0];
-            vd.gd[1] = rz.get(REC_DXY0) + sc.d2[1][0] * vd.v[1] + rz.get(REC_V + 4 + 3) + acc[1][0];
-            vd.gd[2] = acc[2][0] + sc.d2[2][0] * vd.v[2] + s2z[2];
+            /* grad div v: the parts without the z-coupled mixed sums now, those
+             * once plane lp's contributions are in (same association either way) */
+            const T gd0 = sc.d2[0][0] * vd.v[0] + rz.get(REC_V + 2) + rz.get(REC_DXY1);
+            const T gd1 = rz.get(REC_DXY0) + sc.d2[1][0] * vd.v[1] + rz.get(REC_V + 4 + 3);
+            auto finish_gd = [&]() {
+                vd.gd[0] = gd0 + acc[0][0];
+                vd.gd[1] = gd1 + acc[1][0];
+                vd.gd[2] = fma(sc.d2[2][0], vd.v[2], acc[2][0]) + s2z[2];
+            };
+            if constexpr (!LATE_NOW)
+                finish_gd();
 
             HydroToMag<T> hx;
             MagToHydro<T> mx;
@@ -943,9 +922,9 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
              * exchange barrier of the next plane also guards its reuse: in TMEM
              * the unused columns of record slots 0 and 1 of each group, in shared
              * memory two blocks of 15 rows */
-            const uint32_t xslot  = (uint32_t)(lp & 1) * TM::SLOT + XCol<T>::value;
+            const uint32_t xslot  = LC::XCH0 + (uint32_t)(lp & 1) * LC::XCH_W;
             const uint32_t xmine  = tcol + xslot;
-            const uint32_t xother = GROUP == 0 ? tcol + TM::GROUP + xslot : tcol - TM::GROUP + xslot;
+            const uint32_t xother = tother + xslot;
             T* xh = xch + (size_t)(lp & 1) * XROWS * NCELL; /* rows 0..5 */
             T* xm = xh + (size_t)(k1 - k0) * NCELL;         /* rows 6..14 */
             if constexpr (GROUP == 0) {
@@ -956,7 +935,7 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
                     for (int k = k0; k < k1; ++k)
                         xw.set(k - k0, hx.a[k]);
                     __syncwarp();
-                    xt_store6<T>(xmine, xw);
+                    xw.store(xmine);
                 }
                 else {
 #pragma unroll
@@ -968,16 +947,16 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
                 mag_prepare(sd, vd, p, mx);
                 hx.a[H2M_E]       = e_cs;
                 hx.a[H2M_INV_RHO] = e_irh;
-                hx.a[H2M_U + 0]   = t(VTXBUF_UUX, 0, 0, 0);
-                hx.a[H2M_U + 1]   = t(VTXBUF_UUY, 0, 0, 0);
-                hx.a[H2M_U + 2]   = t(VTXBUF_UUZ, 0, 0, 0);
+                hx.a[H2M_U + 0]   = uz.get(0);
+                hx.a[H2M_U + 1]   = uz.get(1);
+                hx.a[H2M_U + 2]   = uz.get(2);
                 if constexpr (XT) {
                     tmem::Words<T, 9> xw;
 #pragma unroll
                     for (int k = 0; k < AC_M2H_COUNT; ++k)
                         xw.set(k, mx.a[k]);
                     __syncwarp();
-                    xt_store9<T>(xmine, xw);
+                    xw.store(xmine);
                 }
                 else {
 #pragma unroll
@@ -985,10 +964,11 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
                         xm[k * NCELL + cell] = mx.a[k];
                 }
             }
-            /* The step's one block barrier: the exchange values are written; every
-             * thread is done with plane lp - 6 (its z taps were read above), whose
-             * ring slot takes plane lp + 2 next; the records stored in this step
-             * and earlier are visible to the other group after it. */
+            /* The step's one block barrier: the exchange values are written; no
+             * thread reads a plane before lp any more (a plane is read in the
+             * step it arrives; z taps come from the queue), so the ring slot of
+             * plane lp - 6 takes plane lp + 2 next; the tensor-memory entries
+             * stored before it are visible to the other group after it. */
             tmem::wait_st();
             tmem::fence_before_sync();
             __syncthreads();
@@ -1006,22 +986,31 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
                 __syncwarp();
                 if constexpr (GROUP == 0) {
                     tmem::Words<T, 9> xw;
-                    xt_load9<T>(xother, xw);
-                    tmem::wait_ld_tied<tmem::Words<T, 9>::W>(xw.w);
+                    xw.load(xother);
+                    tmem::wait_ld();
+                    xw.tie();
 #pragma unroll
                     for (int k = 0; k < AC_M2H_COUNT; ++k)
                         mx.a[k] = xw.get(k);
                 }
                 else {
                     tmem::Words<T, 6> xw;
-                    xt_load6<T>(xother, xw);
-                    tmem::wait_ld_tied<tmem::Words<T, 6>::W>(xw.w);
+                    xw.load(xother);
+                    tmem::wait_ld();
+                    xw.tie();
 #pragma unroll
                     for (int k = k0; k < k1; ++k)
                         hx.a[k] = xw.get(k - k0);
                 }
             }
-            if (active) {
+            if constexpr (LATE_NOW) {
+                inplane();
+                finish_gd();
+            }
+            /* with the late in-plane part the rates are formed by every thread
+             * (one basic block with it); a cell outside the mesh only skips its
+             * stores */
+            if (LATE_NOW || active) {
                 T rr[4], val[4];
                 if constexpr (GROUP == 0) {
                     if constexpr (!XT) {
@@ -1042,7 +1031,7 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
                             hx.a[k] = xh[(k - k0) * NCELL + cell];
                     }
                     mag_rates(sd, vd, mx, hx, p, rr);
-                    if (cfl) {
+                    if (cfl && active) {
                         const T* u = &hx.a[H2M_U];
                         const T* B = &mx.a[M2H_B];
                         cfl_accumulate(u[0] * u[0] + u[1] * u[1] + u[2] * u[2],
@@ -1061,14 +1050,17 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
                         float oh, ol;
                         rk_update_comp(val[k], lo[k], prev[k], prevl[k], rr[k], c, use_prev, oh,
                                        ol);
-                        outp[k][idx] = oh;
-                        outl[k][idx] = ol;
+                        if (active) {
+                            outp[k][idx] = oh;
+                            outl[k][idx] = ol;
+                        }
                     }
                     else {
                         const RkT64 c = {rk.dt, rk.beta, rk.ab};
                         double o;
                         rk_update(val[k], prev[k], rr[k], c, use_prev, o);
-                        outp[k][idx] = o;
+                        if (active)
+                            outp[k][idx] = o;
                     }
                 }
             }
@@ -1090,6 +1082,8 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
             __syncthreads();
             tmem::fence_after_sync();
         }
+        if constexpr (LATE_NOW)
+            tmem::wait_st(); /* the queue entry of plane lp, read in the next step */
     };
 
     /* planes lp = pfirst .. plast in four phases (interior: lp in [z0, z1);

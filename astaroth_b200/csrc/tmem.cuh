@@ -187,6 +187,64 @@ ld32(const uint32_t a, uint32_t* v)
                  );
 }
 
+/* N consecutive columns from a, as the widest shapes first (x32, x16, ... x1). */
+template <int N>
+__device__ __forceinline__ void
+st_n(const uint32_t a, const uint32_t* v)
+{
+    if constexpr (N >= 32) {
+        st32(a, v);
+        st_n<N - 32>(a + 32, v + 32);
+    }
+    else if constexpr (N >= 16) {
+        st16(a, v);
+        st_n<N - 16>(a + 16, v + 16);
+    }
+    else if constexpr (N >= 8) {
+        st8(a, v);
+        st_n<N - 8>(a + 8, v + 8);
+    }
+    else if constexpr (N >= 4) {
+        st4(a, v);
+        st_n<N - 4>(a + 4, v + 4);
+    }
+    else if constexpr (N >= 2) {
+        st2(a, v);
+        st_n<N - 2>(a + 2, v + 2);
+    }
+    else if constexpr (N == 1) {
+        st1(a, v[0]);
+    }
+}
+template <int N>
+__device__ __forceinline__ void
+ld_n(const uint32_t a, uint32_t* v)
+{
+    if constexpr (N >= 32) {
+        ld32(a, v);
+        ld_n<N - 32>(a + 32, v + 32);
+    }
+    else if constexpr (N >= 16) {
+        ld16(a, v);
+        ld_n<N - 16>(a + 16, v + 16);
+    }
+    else if constexpr (N >= 8) {
+        ld8(a, v);
+        ld_n<N - 8>(a + 8, v + 8);
+    }
+    else if constexpr (N >= 4) {
+        ld4(a, v);
+        ld_n<N - 4>(a + 4, v + 4);
+    }
+    else if constexpr (N >= 2) {
+        ld2(a, v);
+        ld_n<N - 2>(a + 2, v + 2);
+    }
+    else if constexpr (N == 1) {
+        ld1(a, v);
+    }
+}
+
 /* Waits for this thread's loads, then ties the loaded words to the wait (an
  * empty volatile statement per word, after the wait in program order) so that
  * no use of them can be scheduled before it. */
@@ -223,6 +281,15 @@ struct Words {
                                                        (unsigned long long)w[2 * i]));
         else
             return (T)__uint_as_float(w[i]);
+    }
+    __device__ __forceinline__ void store(const uint32_t a) const { st_n<W>(a, w); }
+    __device__ __forceinline__ void load(const uint32_t a) { ld_n<W>(a, w); }
+    /* after this thread's wait::ld: ties the words to it */
+    __device__ __forceinline__ void tie()
+    {
+#pragma unroll
+        for (int i = 0; i < W; ++i)
+            asm volatile("" : "+r"(w[i]));
     }
 };
 

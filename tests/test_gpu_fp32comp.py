@@ -52,7 +52,7 @@ def test_load_store_roundtrip_is_hi_plus_lo():
     assert np.abs(out - f).max() <= 2.0 ** -48 * np.abs(f).max()
 
 
-@pytest.mark.parametrize("n", [16, (40, 24, 12)])
+@pytest.mark.parametrize("n", [16, (40, 24, 12), (37, 9, 11), (9, 5, 6)])
 def test_periodic_bitexact_on_pairs(n):
     info = ab.make_info(n, precision=1, **ab.CONFIG_PARAMS)
     f = ab.seeded_mesh(info, 4)

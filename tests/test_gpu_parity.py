@@ -75,7 +75,8 @@ def test_periodic_bitexact_golden(name):
     assert sha(out) == META["cases"][name]["periodic_sha256"]
 
 
-@pytest.mark.parametrize("n", [16, (20, 12, 8), 33])
+# 16-byte-aligned rows, odd rows (alternating 8-byte alignment), small x extents
+@pytest.mark.parametrize("n", [16, (20, 12, 8), 33, (37, 9, 11), (8, 8, 8), (6, 7, 5)])
 def test_periodic_bitexact_oracle(n):
     info = ab.make_info(n, **ab.CONFIG_PARAMS)
     f = ab.seeded_mesh(info, 21)
