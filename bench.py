@@ -315,7 +315,7 @@ def run_gpu(args):
     alg_bytes_step = BYTES_PER_CELL_STEP["fp64"] * cells
     peak, peak_kind = peaks()
     achieved = alg_bytes_step / (solve_step_ms * 1e-3) / 1e9
-    traffic = profile_traffic("solve_tiled_fp64_256.md")
+    traffic = profile_traffic("solve_lead_fp64_256.md")
 
     # ---- e2e through the C ABI with pinned host buffers
     e2e = None
@@ -414,12 +414,12 @@ def run_gpu(args):
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "solve (3 launches per RK3 step)",
                          "alg_bytes_per_launch": alg_bytes_step / 3,
-                         "traffic_source": "profiles/solve_tiled_fp64_256.md (ncu dram bytes at "
+                         "traffic_source": "profiles/solve_lead_fp64_256.md (ncu dram bytes at "
                                            "256^3 scaled by the cell count to 512^3)",
                          "bytes_per_cell_step": BYTES_PER_CELL_STEP["fp64"],
                          "peak_source": peak_kind, "solve_ms_per_step": solve_step_ms,
                          "boundconds_ms_per_step": sum(bc_ms[-3:]),
-                         "limiter": profile_limiter("solve_tiled_fp64_256.md")},
+                         "limiter": profile_limiter("solve_lead_fp64_256.md")},
             "e2e": e2e, "gpu_launches": launches, "clocks": clocks, "cpu_baseline": cpu,
             "fp32comp": fp32, "ensemble": ens, "cfl1024": cfl, "adjoint": adj,
         }
