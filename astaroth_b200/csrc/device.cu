@@ -89,6 +89,8 @@ ac_make_phys(const AcMeshInfo& info, PhysConst* pc)
     pc->upwind       = info.int_params[AC_upwind] != 0;
     pc->debug_skip_load = 0;
     pc->cfl_sum         = info.int_params[AC_additive_timestep] != 0;
+    pc->zlo             = 0;
+    pc->zhi             = info.int3_params[AC_nlocal].z;
     pc->forcing      = 0;
     for (int a = 0; a < 3; ++a)
         pc->f_k[a] = pc->f_re[a] = pc->f_im[a] = 0.0;
@@ -708,17 +710,29 @@ ac_rk_coef(const int step, const double dt)
 
 cudaError_t
 launch_substep(Device d, cudaStream_t st, const int step, const double dt,
-               unsigned long long* launches)
+               unsigned long long* launches, const int zlo, const int zhi)
 {
     StencilCoef sc;
     PhysConst pc;
     ac_make_stencil(d->config, &sc);
     ac_make_phys(d->config, &pc);
     pc.debug_skip_load = d->debug_skip_load;
+    if (zhi >= 0) {
+        pc.zlo = zlo;
+        pc.zhi = zhi;
+    }
+    /* substep 2 in z boxes: the CFL maxima (and B) are set up at the first box,
+     * when the planes solved since the last clear cover the interior */
+    bool first_box = true;
+    if (step == 2) {
+        const bool whole = pc.zlo == 0 && pc.zhi == d->geom.nz;
+        first_box        = whole || d->cfl_cover <= 0 || d->cfl_cover >= d->geom.nz;
+        d->cfl_cover     = (first_box ? 0 : d->cfl_cover) + (pc.zhi - pc.zlo);
+    }
     if (step == 2)
         forcing_for_launch(d->config, dt, &pc);
     const RkCoef rk = ac_rk_coef(step, dt);
-    if (step == 2 && d->config.int_params[AC_lbfield] && d->bfield) {
+    if (step == 2 && first_box && d->config.int_params[AC_lbfield] && d->bfield) {
         /* B = curl A of this substep's input (the in-buffer is not written) */
         const void* a[3];
         double* b[3];
@@ -739,9 +753,11 @@ launch_substep(Device d, cudaStream_t st, const int step, const double dt,
      * reference's calc_timestep inside the third substep (mhdsolver.ac:611) */
     unsigned long long* cfl = nullptr;
     if (step == 2) {
-        const cudaError_t e = cudaMemsetAsync(d->cfl, 0, 3 * sizeof(unsigned long long), st);
-        if (e != cudaSuccess)
-            return e;
+        if (first_box) {
+            const cudaError_t e = cudaMemsetAsync(d->cfl, 0, 3 * sizeof(unsigned long long), st);
+            if (e != cudaSuccess)
+                return e;
+        }
         cfl = d->cfl;
     }
     cudaError_t e;
@@ -795,15 +811,21 @@ acDeviceIntegrateSubstep(const Device d, const Stream stream, const int step_num
 {
     if (!d || !stream_ok(stream) || step_number < 0 || step_number > 2)
         return AC_FAILURE;
-    /* As the reference's default (two-pass) build, device.cc:965-970, only the
-     * whole interior is accepted. */
-    if (!is_whole_interior(d, start, end)) {
-        fprintf(stderr, "astaroth_b200: acDeviceIntegrateSubstep needs start = nmin and "
-                        "end = nmin + nlocal\n");
+    /* The whole interior, as the reference's default (two-pass) build,
+     * device.cc:965-970, or a box of whole interior x-y planes: the singlepass
+     * build solves any box (device.cc:941-964) and its task graph solves the
+     * inner planes while the halos travel (task.cc:1933-1993); z boxes are that
+     * split for the z-slab grid.  The boxes of one substep cover the interior
+     * once; in substep 2 their CFL maxima accumulate from the first box on. */
+    if (!is_z_box(d, start, end)) {
+        fprintf(stderr, "astaroth_b200: acDeviceIntegrateSubstep needs start.xy = nmin.xy, "
+                        "end.xy = nmin.xy + nlocal.xy and nmin.z <= start.z < end.z <= "
+                        "nmin.z + nlocal.z\n");
         return AC_FAILURE;
     }
     AC_CUDA_CHECK(cudaSetDevice(d->id));
-    AC_CUDA_CHECK(launch_substep(d, d->streams[stream], step_number, dt, &d->launches));
+    AC_CUDA_CHECK(launch_substep(d, d->streams[stream], step_number, dt, &d->launches,
+                                 (int)start.z - NGHOST, (int)end.z - NGHOST));
     if (step_number == 2)
         d->out_set = 0;
     return AC_SUCCESS;

@@ -106,9 +106,18 @@ is_whole_interior(const Device d, const Volume start, const Volume end)
            end.z == (size_t)(d->geom.nz + NGHOST);
 }
 
-/* device.cu */
+/* A box of whole interior x-y planes: [nmin.z + zlo, nmin.z + zhi) in z. */
+static inline bool
+is_z_box(const Device d, const Volume start, const Volume end)
+{
+    return start.x == NGHOST && start.y == NGHOST && end.x == (size_t)(d->geom.nx + NGHOST) &&
+           end.y == (size_t)(d->geom.ny + NGHOST) && start.z >= NGHOST && start.z < end.z &&
+           end.z <= (size_t)(d->geom.nz + NGHOST);
+}
+
+/* device.cu; [zlo, zhi) are the interior z planes solved (zhi < 0: all) */
 cudaError_t launch_substep(Device d, cudaStream_t st, const int step, const double dt,
-                           unsigned long long* launches);
+                           unsigned long long* launches, const int zlo = 0, const int zhi = -1);
 cudaError_t launch_periodic(Device d, cudaStream_t st, const int q0, const int nq,
                             const Volume start, const Volume end, unsigned long long* launches);
 void invalidate_tape_graph(Device d);

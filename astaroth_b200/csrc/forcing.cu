@@ -18,12 +18,12 @@ forcing_kernel(const Geom g, T* __restrict__ ux, T* __restrict__ uy, T* __restri
                float* __restrict__ lx, float* __restrict__ ly, float* __restrict__ lz,
                const PhysConst pc)
 {
-    const long long n = (long long)g.nx * g.ny * g.nz;
+    const long long n = (long long)g.nx * g.ny * (pc.zhi - pc.zlo);
     for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x) {
         const int i         = (int)(t % g.nx);
         const int j         = (int)((t / g.nx) % g.ny);
-        const int k         = (int)(t / ((long long)g.nx * g.ny));
+        const int k         = pc.zlo + (int)(t / ((long long)g.nx * g.ny));
         const long long idx = geom_idx(g, i + NGHOST, j + NGHOST, k + NGHOST);
         T f[3];
         forcing_at(pc, i, j, k, f);
@@ -52,7 +52,9 @@ cudaError_t
 ac_launch_forcing(const Geom& g, void* const* u, float* const* lo, const int precision,
                   const PhysConst& pc, cudaStream_t stream, unsigned long long* launches)
 {
-    const long long n = (long long)g.nx * g.ny * g.nz;
+    const long long n = (long long)g.nx * g.ny * (pc.zhi - pc.zlo);
+    if (n <= 0)
+        return cudaSuccess;
     long long blocks  = (n + 255) / 256;
     if (blocks > 148LL * 16)
         blocks = 148LL * 16;

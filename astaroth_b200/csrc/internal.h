@@ -58,6 +58,7 @@ struct PhysConst {
     int upwind;           /* AC_upwind: the LUPWD terms (selects the kernel variant) */
     int debug_skip_load;  /* acDeviceDebugSkipPlaneLoad: the fault-path test of the tiled kernels */
     int cfl_sum;          /* AC_additive_timestep: substep 2 also forms the additive CFL sum */
+    int zlo, zhi;         /* the interior z planes [zlo, zhi) this launch solves */
     /* helical forcing of this launch (substep 2 only; forcing = 0 otherwise):
      * u += scale (re cos(a + phase) - im sin(a + phase)), a = sum_d f_k[d] idx_d
      * with idx the interior cell index (mhdsolver.ac:286-331) */
@@ -169,6 +170,9 @@ struct device_s {
     StepGraph graphs[NUM_STREAMS][2];
     int solve_variant;   /* 0 = plain, else the tiled kernel AC_SOLVE_TILED_* */
     int debug_skip_load; /* acDeviceDebugSkipPlaneLoad */
+    /* planes of substep 2 solved since the CFL maxima were last cleared (a
+     * substep solved in z boxes clears them once, at its first box) */
+    int cfl_cover;
     /* adjoint buffers, allocated by the first acDeviceLoadAdjoint */
     double* adj_lf;      /* 8 fields */
     double* adj_lw;      /* 8 fields */

@@ -26,9 +26,9 @@ solve_plain_kernel(const Geom g, const FieldsT<T> f, const StencilT<T> sc, const
     __shared__ T red[3 * 4];
     const int i = threadIdx.x + blockIdx.x * blockDim.x;
     const int j = threadIdx.y + blockIdx.y * blockDim.y;
-    const int k = blockIdx.z;
+    const int k = pc.zlo + (int)blockIdx.z;
     T cm[3]     = {0, 0, 0};
-    if (i < g.nx && j < g.ny && k < g.nz)
+    if (i < g.nx && j < g.ny && k < pc.zhi)
         plain_cell<T, COMP, UPWD>(g, PtrFieldsT<T>{f}, sc, pc, rk, cfl != nullptr, i, j, k, cm);
     if (cfl)
         cfl_commit(cm, red, cfl);
@@ -41,7 +41,7 @@ launch_plain(const Geom& g, const FieldsT<T>& f, const StencilCoef& sc, const Ph
              unsigned long long* launches)
 {
     const dim3 tpb(32, 4, 1);
-    const dim3 bpg((g.nx + tpb.x - 1) / tpb.x, (g.ny + tpb.y - 1) / tpb.y, g.nz);
+    const dim3 bpg((g.nx + tpb.x - 1) / tpb.x, (g.ny + tpb.y - 1) / tpb.y, pc.zhi - pc.zlo);
     if (pc.upwind)
         solve_plain_kernel<T, COMP, true><<<bpg, tpb, 0, stream>>>(g, f, stencil_cast<T>(sc), pc,
                                                                   rk, cfl);

@@ -244,8 +244,8 @@ solve_tiled_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const
     const int cell  = ly * TX + lx;
     const int x0    = blockIdx.x * TX;
     const int y0    = blockIdx.y * TY;
-    const int z0    = blockIdx.z * zchunk;
-    const int z1    = min(z0 + zchunk, g.nz);
+    const int z0    = pc.zlo + (int)blockIdx.z * zchunk;
+    const int z1    = min(z0 + zchunk, pc.zhi);
     const int pfirst = z0 - NGHOST;     /* first plane needed (interior z index) */
     const int plast  = z1 - 1 + NGHOST; /* last plane needed */
 
@@ -643,8 +643,8 @@ template <typename T, bool COMP, int GROUP, bool XT>
 __device__ __forceinline__ void
 lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const StencilT<T>& sc,
            const PhysT<T>& p, const RkCoef& rk, int* err, unsigned long long* cfl, T* smem, T* xch,
-           T* red, uint64_t* bars, const uint32_t tcol, const int zchunk, const bool skip_last,
-           const bool cfl_sum)
+           T* red, uint64_t* bars, const uint32_t tcol, const int zchunk, const int zlo,
+           const int zhi, const bool skip_last, const bool cfl_sum)
 {
     const long long wlim = skip_last ? kDebugWaitLimit : kWaitLimit;
     typedef Layout<T> L;
@@ -660,8 +660,8 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
     const int cell   = ly * TX + lx;
     const int x0     = blockIdx.x * TX;
     const int y0     = blockIdx.y * TY;
-    const int z0     = blockIdx.z * zchunk;
-    const int z1     = min(z0 + zchunk, g.nz);
+    const int z0     = zlo + (int)blockIdx.z * zchunk;
+    const int z1     = min(z0 + zchunk, zhi);
     const int pfirst = z0 - NGHOST;
     const int plast  = z1 - 1 + NGHOST;
     const int x = x0 + lx, y = y0 + ly;
@@ -1126,8 +1126,8 @@ solve_lead_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const 
     const int warp  = threadIdx.y; /* blockDim.x == 32 */
     const int group = threadIdx.y / TY;
     const int tid   = threadIdx.y * TX + threadIdx.x;
-    const int z0    = blockIdx.z * zchunk;
-    const int z1    = min(z0 + zchunk, g.nz);
+    const int z0    = pc.zlo + (int)blockIdx.z * zchunk;
+    const int z1    = min(z0 + zchunk, pc.zhi);
     const int pfirst = z0 - NGHOST;
     const int plast  = z1 - 1 + NGHOST;
 
@@ -1162,10 +1162,10 @@ solve_lead_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const 
     const StencilT<T> scv   = sc;
     if (group == 0)
         lead_group<T, COMP, 0, XT>(&tmap, g, f, scv, p, rk, err, cfl, smem, xch, red, bars, tcol,
-                               zchunk, skip_last, pc.cfl_sum != 0);
+                               zchunk, pc.zlo, pc.zhi, skip_last, pc.cfl_sum != 0);
     else
         lead_group<T, COMP, 1, XT>(&tmap, g, f, scv, p, rk, err, cfl, smem, xch, red, bars, tcol,
-                               zchunk, skip_last, pc.cfl_sum != 0);
+                               zchunk, pc.zlo, pc.zhi, skip_last, pc.cfl_sum != 0);
     /* no copy into this block's shared memory is left in flight */
     if (tid == 0)
         drain_ring(bars, RING, [&](const int sl) { return loads_into(sl, pfirst, plast, skip_last); });
@@ -1205,11 +1205,11 @@ encode_fn()
  * than two CTAs per SM of the 148.  Every chunk reads 6 halo planes beyond its
  * own, so long chunks are cheaper where the grid is large enough. */
 int
-zchunk_for(const Geom& g)
+zchunk_for(const Geom& g, const int nz)
 {
     const long long tiles = (long long)((g.nx + TX - 1) / TX) * ((g.ny + TY - 1) / TY);
     int zc                = ZCHUNK;
-    while (zc > 8 && tiles * ((g.nz + zc - 1) / zc) < 2 * 148)
+    while (zc > 8 && tiles * ((nz + zc - 1) / zc) < 2 * 148)
         zc /= 2;
     return zc;
 }
@@ -1221,13 +1221,21 @@ launch_tiled(const Geom& g, const void* tmap_in, const FieldsT<T>& f, const Sten
              cudaStream_t stream, unsigned long long* launches, const int kernel)
 {
     const dim3 tpb(TX, 2 * TY, 1);
-    const int zc = zchunk_for(g);
-    const dim3 bpg((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (g.nz + zc - 1) / zc);
+    /* the planes [zlo, zhi) of this launch (all nz unless the caller solves the
+     * interior in z boxes) */
+    const int nzr = pc.zhi - pc.zlo;
+    if (nzr <= 0)
+        return cudaSuccess;
+    const int zc = zchunk_for(g, nzr);
+    const dim3 bpg((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (nzr + zc - 1) / zc);
     /* The leading-plane kernel forms stage 1 for the 6 halo planes of every z
      * chunk too; on short chunks (small meshes) that overhead loses to the
-     * per-plane tap kernel, so the automatic choice takes it from 32 planes. */
+     * per-plane tap kernel, so the automatic choice takes it from 32 planes.
+     * The choice follows the whole mesh, so that a substep solved in z boxes
+     * gives the bits of the whole-interior launch (the results of either kernel
+     * do not depend on where the z chunks start). */
     const int k = kernel == AC_SOLVE_TILED_AUTO
-                      ? (zc >= 32 ? AC_SOLVE_TILED_LEAD : AC_SOLVE_TILED_TAPS)
+                      ? (zchunk_for(g, g.nz) >= 32 ? AC_SOLVE_TILED_LEAD : AC_SOLVE_TILED_TAPS)
                       : kernel;
     if (pc.upwind)
         solve_tiled_kernel<T, COMP, true><<<bpg, tpb, Layout<T>::SMEM_BYTES, stream>>>(

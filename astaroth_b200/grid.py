@@ -14,6 +14,18 @@ One RK3 substep of the grid is, on every slab:
    buffer, a transport, acDeviceUnpackPlanes into the ghost planes;
 3. acDeviceIntegrateSubstep and the buffer swap.
 
+With ``overlap`` and every slab at least 7 planes deep, step 3 overlaps step
+2, as the reference's task graph does (src/core/task.cc:1933-1993): each slab
+solves its interior planes [3, n - 3), which read no ghost plane, on its second
+library stream as soon as the x/y fill is done, while the planes travel on the
+first; after the unpack the first stream waits for that solve and solves the
+three planes at each end (acDeviceIntegrateSubstep on z boxes).  The default
+overlaps where the planes cross between GPUs (DistTransport with more than one
+rank).  With every slab on one GPU (LocalTransport) the exchange is a copy in
+the same HBM and there is nothing to hide: measured on one B200, the split
+substep is 3-9% slower than the serial one (two more launches per substep and
+slab, and the end boxes load 9 planes for 3).
+
 Transports:
 
 * ``LocalTransport`` -- every slab in this process, on one GPU; the exchange
@@ -162,7 +174,8 @@ class Grid:
     this process holds its rank's slab of ``world`` slabs.
     """
 
-    def __init__(self, info: AcMeshInfo, slabs: int = 1, transport=None, device_id: int = 0):
+    def __init__(self, info: AcMeshInfo, slabs: int = 1, transport=None, device_id: int = 0,
+                 overlap: bool | None = None):
         import torch
 
         self.lib = capi.load()
@@ -180,6 +193,12 @@ class Grid:
         dev = torch.device("cuda", device_id)
         self._streams = [torch.cuda.ExternalStream(d.stream_handle(0), device=dev)
                          for d in self.devs]
+        # the interior solve of the overlapped substep runs on library stream 1
+        self._streams1 = [torch.cuda.ExternalStream(d.stream_handle(1), device=dev)
+                          for d in self.devs]
+        if overlap is None:
+            overlap = isinstance(transport, DistTransport) and transport.world > 1
+        self.overlap = overlap and min(n for _, n in self.ranges) >= 2 * HALO + 1
         self._buf = {k: [torch.empty(HALO * self.plane_bytes, dtype=torch.uint8, device=dev)
                          for _ in self.devs] for k in ("sb", "st", "rb", "rt")}
         self.cells = self.n[0] * self.n[1] * self.n[2]
@@ -212,16 +231,23 @@ class Grid:
         return out
 
     # ---- boundary conditions ----
-    def periodic_boundconds(self) -> None:
+    def periodic_boundconds(self, interior_step=None) -> None:
         """Fills every ghost cell of every slab: x and y by local wrap, z by the
         exchange with the neighbouring slabs.  Everything is ordered on the
-        slabs' library streams (stream 0); the host does not wait."""
+        slabs' library streams (stream 0); the host does not wait.
+
+        interior_step: (step, dt) of a substep whose interior planes each slab
+        solves on its stream 1 once its x/y fill is done, while the planes
+        travel (the overlapped substep)."""
         b = self._buf
+        nx, ny, _ = self.n
         for i, (d, (_, n)) in enumerate(zip(self.devs, self.ranges)):
-            nx, ny, _ = self.n
             _check(self.lib.acDevicePeriodicBoundconds(
                 d.handle, 0, Volume(0, 0, HALO), Volume(nx + 2 * HALO, ny + 2 * HALO, n + HALO)),
                 "acDevicePeriodicBoundconds")
+            if interior_step is not None:
+                self._streams1[i].wait_stream(self._streams[i])
+                self._solve_box(d, 1, interior_step, 2 * HALO, n)
             _check(self.lib.acDevicePackPlanes(d.handle, 0, HALO, HALO, b["sb"][i].data_ptr()),
                    "acDevicePackPlanes")
             _check(self.lib.acDevicePackPlanes(d.handle, 0, n, HALO, b["st"][i].data_ptr()),
@@ -233,11 +259,32 @@ class Grid:
             _check(self.lib.acDeviceUnpackPlanes(d.handle, 0, n + HALO, HALO,
                                                  b["rt"][i].data_ptr()), "acDeviceUnpackPlanes")
 
+    def _solve_box(self, d, stream: int, step_dt, z0: int, z1: int) -> None:
+        """acDeviceIntegrateSubstep on the interior x-y planes [z0, z1) (padded
+        z indices) of slab device d."""
+        nx, ny, _ = self.n
+        step, dt = step_dt
+        _check(self.lib.acDeviceIntegrateSubstep(d.handle, stream, step, Volume(HALO, HALO, z0),
+                                                 Volume(nx + HALO, ny + HALO, z1), dt),
+               "acDeviceIntegrateSubstep")
+
     # ---- integration ----
     def integrate_substep(self, step: int, dt: float) -> None:
-        self.periodic_boundconds()
-        for d in self.devs:
-            d.integrate_substep(step, dt)
+        if not self.overlap:
+            self.periodic_boundconds()
+            for d in self.devs:
+                d.integrate_substep(step, dt)
+            for d in self.devs:
+                d.swap_buffers()
+            return
+        # interior planes while the boundary planes travel; then, after the
+        # unpack and the interior solve (whose first box also clears the CFL
+        # maxima of substep 2), the three planes at each end
+        self.periodic_boundconds(interior_step=(step, dt))
+        for i, (d, (_, n)) in enumerate(zip(self.devs, self.ranges)):
+            self._streams[i].wait_stream(self._streams1[i])
+            self._solve_box(d, 0, (step, dt), HALO, 2 * HALO)
+            self._solve_box(d, 0, (step, dt), n, n + HALO)
         for d in self.devs:
             d.swap_buffers()
 

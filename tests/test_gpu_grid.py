@@ -32,23 +32,97 @@ def _interior(a):
     return a[:, 3:-3, 3:-3, 3:-3]
 
 
+# overlap: the interior planes solved while the planes travel, then the ends
+@pytest.mark.parametrize("overlap", [False, True])
 @pytest.mark.parametrize("kernel", [0, 3])  # the default choice; the leading-plane kernel
 @pytest.mark.parametrize("precision", [0, 1])
 @pytest.mark.parametrize("shape,slabs", [((40, 36, 48), 2), ((32, 32, 20), 3), ((40, 36, 48), 4),
                                          ((33, 24, 16), 1)])
-def test_slabs_equal_one_device(shape, slabs, precision, kernel):
+def test_slabs_equal_one_device(shape, slabs, precision, kernel, overlap):
     if kernel == 3 and (precision == 0 and shape[0] % 2):
         pytest.skip("odd nx in FP64 takes the plain kernel")
     info = make_info(shape, precision=precision)
     info.int_params[IntParam.AC_debug_plain_kernel] = kernel
     f = seeded_mesh(info, 81)
-    with Grid(info, slabs=slabs) as g:
+    with Grid(info, slabs=slabs, overlap=overlap) as g:
+        # slabs of fewer than 7 planes have no interior box: the serial substep
+        assert g.overlap == (overlap and min(n for _, n in g.ranges) >= 7)
         g.load_mesh(f)
         for _ in range(3):
             g.integrate_step(DT)
         g.synchronize()
         got = g.store_mesh()
     assert np.array_equal(_interior(got), _interior(_device(info, f, 3)))
+
+
+def _boxes_run(info, f, boxes, forcing=False):
+    """Three RK3 steps, each substep as acDeviceIntegrateSubstep on the z boxes
+    (padded z ranges) in order; the final mesh and the CFL timestep."""
+    lib = capi.load()
+    n = info.int3_params[capi.Int3Param.AC_nlocal]
+    nx, ny = n.x, n.y
+    h = capi.NGHOST
+    with Device(info) as d:
+        d.load_mesh(f)
+        for _ in range(3):
+            for s in range(3):
+                d.periodic_boundconds()
+                for z0, z1 in boxes:
+                    assert lib.acDeviceIntegrateSubstep(d.handle, 0, s, capi.Volume(h, h, z0),
+                                                        capi.Volume(nx + h, ny + h, z1),
+                                                        DT) == capi.AC_SUCCESS
+                d.swap_buffers()
+        d.synchronize()
+        return d.store_mesh(), d.timestep()
+
+
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_substep_in_z_boxes_equals_whole(precision, kernel):
+    """acDeviceIntegrateSubstep on z boxes -- the interior planes, then the three
+    at each end, as the overlapped grid substep calls it -- gives the bits of the
+    whole-interior call with every kernel, and substep 2's CFL maxima cover all
+    boxes (the first box clears them)."""
+    shape = (64, 40, 72)
+    info = make_info(shape, precision=precision)
+    info.int_params[IntParam.AC_debug_plain_kernel] = kernel
+    f = seeded_mesh(info, 86, sigma_uu=1e-2)
+    h, nz = capi.NGHOST, shape[2]
+    whole, whole_dt = _boxes_run(info, f, [(h, nz + h)])
+    split, split_dt = _boxes_run(info, f, [(2 * h, nz), (h, 2 * h), (nz, nz + h)])
+    assert np.array_equal(split, whole)
+    assert split_dt == whole_dt
+    # the boxes may come in any order (here the top first)
+    split2, split2_dt = _boxes_run(info, f, [(nz, nz + h), (2 * h, nz), (h, 2 * h)])
+    assert np.array_equal(split2, whole)
+    assert split2_dt == whole_dt
+
+
+def test_substep_z_boxes_with_forcing():
+    """With helical forcing on, each box forces its own planes once."""
+    info = make_info((32, 32, 24), **dict(CONFIG_PARAMS, relhel=0.5, forcing_magnitude=0.5,
+                                           kmin=0.8, kmax=2.2, current_time=1.0))
+    info.int_params[IntParam.AC_lforcing] = 1
+    assert capi.load().acHostForcingParams(Real3(1, 0, 1), 0.4, 0.7, C.byref(info)) == 0
+    f = seeded_mesh(info, 88)
+    h, nz = capi.NGHOST, 24
+    whole, _ = _boxes_run(info, f, [(h, nz + h)])
+    split, _ = _boxes_run(info, f, [(2 * h, nz), (h, 2 * h), (nz, nz + h)])
+    assert np.array_equal(split, whole)
+
+
+def test_substep_rejects_partial_xy_boxes():
+    info = make_info((32, 32, 24))
+    lib = capi.load()
+    h = capi.NGHOST
+    with Device(info) as d:
+        for start, end in (((h + 1, h, h), (32 + h, 32 + h, 24 + h)),
+                           ((h, h, h), (32 + h, 31 + h, 24 + h)),
+                           ((h, h, h - 1), (32 + h, 32 + h, 24 + h)),
+                           ((h, h, 10), (32 + h, 32 + h, 10)),
+                           ((h, h, h), (32 + h, 32 + h, 25 + h))):
+            assert lib.acDeviceIntegrateSubstep(d.handle, 0, 0, capi.Volume(*start),
+                                                capi.Volume(*end), DT) == capi.AC_FAILURE
 
 
 @pytest.mark.parametrize("precision", [0, 1])
@@ -69,7 +143,8 @@ def test_slabs_with_upwinding(precision):
 def test_reductions_and_timestep():
     info = make_info((40, 36, 30))
     f = seeded_mesh(info, 82, sigma_uu=1e-2)
-    with Grid(info, slabs=3) as g, Device(info) as d:
+    with Grid(info, slabs=3, overlap=True) as g, Device(info) as d:
+        assert g.overlap
         g.load_mesh(f)
         d.load_mesh(f)
         g.integrate_step(DT)
@@ -90,7 +165,8 @@ def test_forcing_across_slabs():
     info.int_params[IntParam.AC_lforcing] = 1
     assert capi.load().acHostForcingParams(Real3(1, 0, 1), 0.4, 0.7, C.byref(info)) == 0
     f = seeded_mesh(info, 83)
-    with Grid(info, slabs=3) as g:
+    with Grid(info, slabs=3, overlap=True) as g:
+        assert g.overlap
         g.load_mesh(f)
         g.integrate_step(DT)
         g.synchronize()
@@ -112,7 +188,8 @@ def test_dist_transport_one_rank():
     try:
         info = make_info((32, 28, 24))
         f = seeded_mesh(info, 84)
-        with Grid(info, transport=DistTransport()) as g:
+        with Grid(info, transport=DistTransport(), overlap=True) as g:
+            assert g.overlap
             g.load_mesh(f)
             for _ in range(2):
                 g.integrate_step(DT)

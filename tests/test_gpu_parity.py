@@ -309,7 +309,7 @@ def test_api_errors_and_state():
     info = ab.make_info(16, **ab.CONFIG_PARAMS)
     lib = capi.load()
     with ab.Device(info) as dev:
-        # substeps accept only the whole interior and steps 0..2
+        # substeps accept boxes of whole interior x-y planes and steps 0..2
         bad = capi.Volume(4, 3, 3)
         assert lib.acDeviceIntegrateSubstep(dev.handle, 0, 0, bad, dev.vols.n1, 1e-3) == 1
         assert lib.acDeviceIntegrateSubstep(dev.handle, 0, 3, dev.vols.n0, dev.vols.n1, 1e-3) == 1
