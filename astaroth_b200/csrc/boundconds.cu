@@ -51,13 +51,26 @@ copy_wrapped(const Geom& g, const ArrayList<T>& fl, const int i, const int j, co
  * per row; the others fill the six x ghosts of the interior rows, one thread
  * per row.  Sources (interior cells) and destinations (ghost cells) never
  * overlap, so each thread issues its loads before its stores.  blockIdx.y is
- * the array. */
-template <typename T>
+ * the array.
+ *
+ * VEC (every row and array 16-byte aligned): the ghost rows move as 16-byte
+ * vectors of the row pitch, a vector inside the x interior straight from the
+ * same place of the source row, one with x ghosts (or FP32 row padding, which
+ * takes the source row's) element by element; in FP64 with nx even the x
+ * ghosts of an interior row move as two 16-byte pairs and two single cells.
+ * Half the memory instructions of the 8-byte form (the kernel is bound by the
+ * queue of outstanding memory instructions). */
+template <typename T, bool VEC>
 __global__ void __launch_bounds__(256)
 periodic_rows_kernel(const Geom g, const ArrayList<T> fl, const int blocks_rows)
 {
     T* a         = fl.p[blockIdx.y];
     const int nx = g.nx, ny = g.ny, nz = g.nz, mx = g.mx, my = g.my;
+    constexpr int W = 16 / (int)sizeof(T); /* elements per 16-byte vector */
+    union Vec {
+        uint4 u;
+        T v[W];
+    };
     if ((int)blockIdx.x < blocks_rows) {
         /* ghost rows: the 6 ghost z planes (my rows each), then the 6 ghost y
          * rows of each interior z plane */
@@ -81,6 +94,38 @@ periodic_rows_kernel(const Geom g, const ArrayList<T> fl, const int blocks_rows)
         const int ks = (k - NGHOST + nz) % nz + NGHOST;
         T* dst       = a + geom_idx(g, 0, j, k);
         const T* src = a + geom_idx(g, 0, js, ks);
+        if constexpr (VEC) {
+            constexpr int U = 4; /* vectors in flight per lane */
+            const int nv    = g.px / W;
+            for (int v0 = lane; v0 < nv; v0 += 32 * U) {
+                Vec w[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int v = v0 + 32 * u;
+                    if (v >= nv)
+                        continue;
+                    const int e = v * W;
+                    if (e >= NGHOST && e + W <= nx + NGHOST) {
+                        w[u].u = *reinterpret_cast<const uint4*>(src + e);
+                    }
+                    else {
+#pragma unroll
+                        for (int i = 0; i < W; ++i) {
+                            const int x  = e + i;
+                            const int xs = x < NGHOST ? x + nx : x >= nx + NGHOST && x < mx ? x - nx : x;
+                            w[u].v[i]    = src[xs];
+                        }
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int v = v0 + 32 * u;
+                    if (v < nv)
+                        *reinterpret_cast<uint4*>(dst + v * W) = w[u].u;
+                }
+            }
+            return;
+        }
         constexpr int B = 8; /* loads in flight per lane */
         for (int x0 = lane; x0 < mx; x0 += 32 * B) {
             T v[B];
@@ -107,6 +152,21 @@ periodic_rows_kernel(const Geom g, const ArrayList<T> fl, const int blocks_rows)
         const int k = NGHOST + row / ny;
         const int j = NGHOST + row - (row / ny) * ny;
         T* rp       = a + geom_idx(g, 0, j, k);
+        if constexpr (VEC && sizeof(T) == 8) {
+            if ((nx & 1) == 0) {
+                /* (0, 1) <- (nx, nx + 1), 2 <- nx + 2, nx + 3 <- 3,
+                 * (nx + 4, nx + 5) <- (4, 5): the pairs 16-byte aligned */
+                const uint4 lo = *reinterpret_cast<const uint4*>(rp + nx);
+                const T s2     = rp[nx + 2];
+                const T s3     = rp[NGHOST];
+                const uint4 hi = *reinterpret_cast<const uint4*>(rp + NGHOST + 1);
+                *reinterpret_cast<uint4*>(rp) = lo;
+                rp[2]                         = s2;
+                rp[nx + NGHOST]               = s3;
+                *reinterpret_cast<uint4*>(rp + nx + NGHOST + 1) = hi;
+                return;
+            }
+        }
         T v[6];
 #pragma unroll
         for (int c = 0; c < NGHOST; ++c) {
@@ -315,8 +375,16 @@ ac_launch_periodic(const Geom& g, T* const* arrays, const int n, const Volume st
         const long long b_cells    = (irows + 255) / 256;
         if (b_rows + b_cells > 0x7fffffffLL)
             return cudaErrorInvalidValue;
-        periodic_rows_kernel<T><<<dim3((unsigned)(b_rows + b_cells), (unsigned)n), 256, 0,
-                                  stream>>>(g, fl, (int)b_rows);
+        /* the 16-byte form needs every row (pitch) and array 16-byte aligned */
+        bool vec = ((long long)g.px * (long long)sizeof(T)) % 16 == 0;
+        for (int q = 0; q < n; ++q)
+            vec = vec && ((uintptr_t)arrays[q] & 15) == 0;
+        if (vec)
+            periodic_rows_kernel<T, true><<<dim3((unsigned)(b_rows + b_cells), (unsigned)n), 256,
+                                            0, stream>>>(g, fl, (int)b_rows);
+        else
+            periodic_rows_kernel<T, false><<<dim3((unsigned)(b_rows + b_cells), (unsigned)n), 256,
+                                             0, stream>>>(g, fl, (int)b_rows);
     }
     else {
         const int3 s = make_int3((int)start.x, (int)start.y, (int)start.z);
