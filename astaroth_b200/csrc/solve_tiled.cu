@@ -45,7 +45,7 @@ constexpr int TX     = 32;
 constexpr int TY     = 4;
 constexpr int HY     = TY + 2 * NGHOST;
 constexpr int RING   = 8;
-constexpr int ZCHUNK = 64;
+constexpr int ZCHUNK = 128;
 constexpr int NCELL  = TX * TY; /* cells per tile, one per thread of a group */
 constexpr int XCHG   = (AC_H2M_COUNT + AC_M2H_COUNT) * NCELL; /* exchange entries */
 
