@@ -45,7 +45,7 @@ constexpr int TX     = 32;
 constexpr int TY     = 4;
 constexpr int HY     = TY + 2 * NGHOST;
 constexpr int RING   = 8;
-constexpr int ZCHUNK = 128;
+constexpr int ZCHUNK = 256; /* the longest z chunk (zchunk_for) */
 constexpr int NCELL  = TX * TY; /* cells per tile, one per thread of a group */
 constexpr int XCHG   = (AC_H2M_COUNT + AC_M2H_COUNT) * NCELL; /* exchange entries */
 
@@ -1201,14 +1201,34 @@ encode_fn()
     return fn;
 }
 
-/* Planes per CTA: ZCHUNK, halved (down to 8) while the grid would have fewer
- * than two CTAs per SM of the 148.  Every chunk reads 6 halo planes beyond its
- * own, so long chunks are cheaper where the grid is large enough. */
+/* Planes per CTA.  Every chunk reads and forms 6 halo planes beyond its own,
+ * so long chunks are cheaper, until the grid quantises badly into waves of
+ * resident CTAs.  Among 256, 128, 64 and 32 planes that keep at least two CTAs
+ * per SM of the 148, the chunk with the least (waves of `per_sm` resident CTAs
+ * per SM) x (planes a CTA steps through) is taken; the larger on a tie.
+ * Smaller grids halve 32 down to 8 while there are fewer than two CTAs per SM.
+ * (Measured at 512^3, FP64: 256 planes 29.3 ms per step, 128 planes 29.6-29.8,
+ * 64 planes 30.9; at 256^3, 256-plane chunks would leave 512 CTAs, 3.5 waves.) */
 int
-zchunk_for(const Geom& g, const int nz)
+zchunk_for(const Geom& g, const int nz, const int per_sm)
 {
     const long long tiles = (long long)((g.nx + TX - 1) / TX) * ((g.ny + TY - 1) / TY);
-    int zc                = ZCHUNK;
+    const long long slots = 148LL * per_sm;
+    int best              = 0;
+    long long best_cost   = 0;
+    for (int zc = ZCHUNK; zc >= 32; zc /= 2) {
+        const long long ctas = tiles * ((nz + zc - 1) / zc);
+        if (ctas < 2 * 148)
+            continue;
+        const long long cost = (ctas + slots - 1) / slots * (long long)(min(zc, nz) + 2 * NGHOST);
+        if (best == 0 || cost < best_cost) {
+            best      = zc;
+            best_cost = cost;
+        }
+    }
+    if (best)
+        return best;
+    int zc = 32;
     while (zc > 8 && tiles * ((nz + zc - 1) / zc) < 2 * 148)
         zc /= 2;
     return zc;
@@ -1226,7 +1246,8 @@ launch_tiled(const Geom& g, const void* tmap_in, const FieldsT<T>& f, const Sten
     const int nzr = pc.zhi - pc.zlo;
     if (nzr <= 0)
         return cudaSuccess;
-    const int zc = zchunk_for(g, nzr);
+    const int per_sm = Tile<T>::MINB; /* resident CTAs per SM */
+    const int zc     = zchunk_for(g, nzr, per_sm);
     const dim3 bpg((g.nx + TX - 1) / TX, (g.ny + TY - 1) / TY, (nzr + zc - 1) / zc);
     /* The leading-plane kernel forms stage 1 for the 6 halo planes of every z
      * chunk too; on short chunks (small meshes) that overhead loses to the
@@ -1235,7 +1256,8 @@ launch_tiled(const Geom& g, const void* tmap_in, const FieldsT<T>& f, const Sten
      * gives the bits of the whole-interior launch (the results of either kernel
      * do not depend on where the z chunks start). */
     const int k = kernel == AC_SOLVE_TILED_AUTO
-                      ? (zchunk_for(g, g.nz) >= 32 ? AC_SOLVE_TILED_LEAD : AC_SOLVE_TILED_TAPS)
+                      ? (zchunk_for(g, g.nz, per_sm) >= 32 ? AC_SOLVE_TILED_LEAD
+                                                            : AC_SOLVE_TILED_TAPS)
                       : kernel;
     if (pc.upwind)
         solve_tiled_kernel<T, COMP, true><<<bpg, tpb, Layout<T>::SMEM_BYTES, stream>>>(
