@@ -690,13 +690,20 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
 #pragma unroll
         for (int j = 0; j < 7; ++j)
             acc[a][j] = 0;
+    /* the RK coefficients of the update, converted once */
+    const RkT32 c32 = {(float)rk.dt, (float)rk.beta, (float)rk.ab};
+    const RkT64 c64 = {rk.dt, rk.beta, rk.ab};
+    /* plane lp mod 3 (record slot) and zq_entry(lp), stepped with lp (lp >= -3) */
+    uint32_t r3 = (uint32_t)(pfirst + 3) % 3u;
+    uint32_t q7 = zq_entry(pfirst);
 
     auto step = [&](auto ph, const int lp) {
         constexpr bool INTERIOR = decltype(ph)::interior;
         constexpr bool SOLVE    = decltype(ph)::solve;
         const int z             = lp - NGHOST; /* the plane solved in this step */
         const long long idx     = geom_idx(g, x + NGHOST, y + NGHOST, z + NGHOST);
-        T prev[4] = {0, 0, 0, 0}, prevl[4] = {0, 0, 0, 0}, lo[4] = {0, 0, 0, 0};
+        /* read only where set: active cells, and prev only after substep 0 */
+        T prev[4], prevl[4], lo[4];
         if constexpr (SOLVE) {
             if (active) {
 #pragma unroll
@@ -724,7 +731,7 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
         tmem::Words<T, NREC> rz;
         tmem::Words<T, 1> eo, ro;
         if constexpr (SOLVE) {
-            rz.load(tcol + ((uint32_t)z % 3u) * LC::REC_W);
+            rz.load(tcol + r3 * LC::REC_W); /* z mod 3 = lp mod 3 */
             eo.load(tcol + LC::EXP0 + (uint32_t)(z & 3) * LC::WE);
             ro.load(tother + LC::EXP0 + (uint32_t)(z & 3) * LC::WE);
         }
@@ -742,7 +749,7 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
         for (int c = 0; c < 3; ++c)
             cur.set(c, pl[(Q0 + c) * L::PLANE]);
         {
-            const uint32_t qa = tcol + LC::ZQ0 + zq_entry(lp) * LC::ZQ_E;
+            const uint32_t qa = tcol + LC::ZQ0 + q7 * LC::ZQ_E;
             cur.store(qa);
             cur.store(qa + 7 * LC::ZQ_E);
         }
@@ -813,7 +820,7 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
                 eo.tie();
                 ro.tie();
             }
-            r.store(tcol + ((uint32_t)lp % 3u) * LC::REC_W);
+            r.store(tcol + r3 * LC::REC_W);
         }
         else {
             /* halo planes only feed the mixed sums */
@@ -844,10 +851,12 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
             /* planes z-3 .. z+2 of the vector from the queue (z+3 = lp is cur);
              * the magnetic group also takes u at plane z from the hydro group's */
             tmem::Words<T, 18> win;
-            win.load(tcol + LC::ZQ0 + zq_entry(z - NGHOST) * LC::ZQ_E);
+            /* zq_entry(z - 3) = zq_entry(lp) + 1, zq_entry(z) = zq_entry(lp) + 4 (mod 7) */
+            const uint32_t qw = q7 == 6u ? 0u : q7 + 1u;
+            win.load(tcol + LC::ZQ0 + qw * LC::ZQ_E);
             [[maybe_unused]] tmem::Words<T, 3> uz;
             if constexpr (GROUP == 1)
-                uz.load(tother + LC::ZQ0 + zq_entry(z) * LC::ZQ_E);
+                uz.load(tother + LC::ZQ0 + (q7 >= 3u ? q7 - 3u : q7 + 4u) * LC::ZQ_E);
             T sz1, sz2;
             {
                 const T* c = sc.d1[2];
@@ -1046,9 +1055,8 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     if constexpr (COMP) {
-                        const RkT32 c = {(float)rk.dt, (float)rk.beta, (float)rk.ab};
                         float oh, ol;
-                        rk_update_comp(val[k], lo[k], prev[k], prevl[k], rr[k], c, use_prev, oh,
+                        rk_update_comp(val[k], lo[k], prev[k], prevl[k], rr[k], c32, use_prev, oh,
                                        ol);
                         if (active) {
                             outp[k][idx] = oh;
@@ -1056,9 +1064,8 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
                         }
                     }
                     else {
-                        const RkT64 c = {rk.dt, rk.beta, rk.ab};
                         double o;
-                        rk_update(val[k], prev[k], rr[k], c, use_prev, o);
+                        rk_update(val[k], prev[k], rr[k], c64, use_prev, o);
                         if (active)
                             outp[k][idx] = o;
                     }
@@ -1084,6 +1091,8 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
         }
         if constexpr (LATE_NOW)
             tmem::wait_st(); /* the queue entry of plane lp, read in the next step */
+        r3 = r3 == 2u ? 0u : r3 + 1u;
+        q7 = q7 == 6u ? 0u : q7 + 1u;
     };
 
     /* planes lp = pfirst .. plast in four phases (interior: lp in [z0, z1);
