@@ -668,6 +668,9 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
     const bool active   = x < g.nx && y < g.ny;
     const bool use_prev = rk.step > 0;
     const int cell_off  = (ly + NGHOST) * L::HXP + (lx + NGHOST);
+    /* a cell outside the mesh (its stores are skipped) reads at the nearest cell
+     * of the mesh, so that its loads need no branch */
+    const int xg = min(x, g.nx - 1) + NGHOST, yg = min(y, g.ny - 1) + NGHOST;
     T* outp[4];
     T* outl[4];
     const T* inl[4];
@@ -701,20 +704,18 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
         constexpr bool INTERIOR = decltype(ph)::interior;
         constexpr bool SOLVE    = decltype(ph)::solve;
         const int z             = lp - NGHOST; /* the plane solved in this step */
-        const long long idx     = geom_idx(g, x + NGHOST, y + NGHOST, z + NGHOST);
-        /* read only where set: active cells, and prev only after substep 0 */
+        const long long idx     = geom_idx(g, xg, yg, z + NGHOST);
+        /* prev only after substep 0 */
         T prev[4], prevl[4], lo[4];
         if constexpr (SOLVE) {
-            if (active) {
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
+            for (int k = 0; k < 4; ++k) {
+                if (use_prev)
+                    prev[k] = outp[k][idx];
+                if (COMP) {
+                    lo[k] = inl[k][idx];
                     if (use_prev)
-                        prev[k] = outp[k][idx];
-                    if (COMP) {
-                        lo[k] = inl[k][idx];
-                        if (use_prev)
-                            prevl[k] = outl[k][idx];
-                    }
+                        prevl[k] = outl[k][idx];
                 }
             }
         }
