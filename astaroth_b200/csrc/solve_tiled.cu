@@ -639,7 +639,19 @@ struct LeadPhase {
 /* The whole chunk for the threads of one warp group (GROUP 0: lnrho and uu,
  * GROUP 1: aa and entropy).  Both groups take the same barriers in the same
  * order. */
-template <typename T, bool COMP, int GROUP, bool XT>
+/* MODE: which of the substep's options are fixed at compile time.
+ * MODE_FIRST is substep 0 (no previous state read, no CFL maxima); MODE_RUNTIME
+ * takes both from rk.step and the cfl pointer.  (Forms fixed for substeps 1
+ * and 2 were measured too: in FP64 they take 228-230 registers against 224
+ * and ran 2-3% slower; in FP32 they were even.) */
+enum {
+    MODE_FIRST   = 0,
+    MODE_PREV    = 1,
+    MODE_PREVCFL = 2,
+    MODE_RUNTIME = 3
+};
+
+template <typename T, bool COMP, int GROUP, bool XT, int MODE>
 __device__ __forceinline__ void
 lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const StencilT<T>& sc,
            const PhysT<T>& p, const RkCoef& rk, int* err, unsigned long long* cfl, T* smem, T* xch,
@@ -666,7 +678,8 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
     const int plast  = z1 - 1 + NGHOST;
     const int x = x0 + lx, y = y0 + ly;
     const bool active   = x < g.nx && y < g.ny;
-    const bool use_prev = rk.step > 0;
+    const bool use_prev = MODE == MODE_RUNTIME ? rk.step > 0 : MODE != MODE_FIRST;
+    const bool do_cfl   = MODE == MODE_RUNTIME ? cfl != nullptr : MODE == MODE_PREVCFL;
     const int cell_off  = (ly + NGHOST) * L::HXP + (lx + NGHOST);
     /* a cell outside the mesh (its stores are skipped) reads at the nearest cell
      * of the mesh, so that its loads need no branch */
@@ -1041,7 +1054,7 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
                             hx.a[k] = xh[(k - k0) * NCELL + cell];
                     }
                     mag_rates(sd, vd, mx, hx, p, rr);
-                    if (cfl && active) {
+                    if (do_cfl && active) {
                         const T* u = &hx.a[H2M_U];
                         const T* B = &mx.a[M2H_B];
                         cfl_accumulate(u[0] * u[0] + u[1] * u[1] + u[2] * u[2],
@@ -1110,7 +1123,7 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
     for (; lp <= plast; ++lp)
         step(LeadPhase<false, true>{}, lp);
 
-    if (cfl) {
+    if (do_cfl) {
         __syncthreads(); /* every thread's last exchange reads are done */
         cfl_commit(cm, red, cfl);
     }
@@ -1118,7 +1131,7 @@ lead_group(const CUtensorMap* tmap, const Geom& g, const FieldsT<T>& f, const St
         atomicExch(err, 1);
 }
 
-template <typename T, bool COMP, bool XT>
+template <typename T, bool COMP, bool XT, int MODE>
 __global__ void __launch_bounds__(2 * TX * TY, Tile<T>::MINB)
 solve_lead_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const FieldsT<T> f,
                   const StencilT<T> sc, const PhysConst pc, const RkCoef rk, int* err,
@@ -1171,10 +1184,10 @@ solve_lead_kernel(const __grid_constant__ CUtensorMap tmap, const Geom g, const 
     const PhysT<T> p        = phys_cast<T>(pc);
     const StencilT<T> scv   = sc;
     if (group == 0)
-        lead_group<T, COMP, 0, XT>(&tmap, g, f, scv, p, rk, err, cfl, smem, xch, red, bars, tcol,
+        lead_group<T, COMP, 0, XT, MODE>(&tmap, g, f, scv, p, rk, err, cfl, smem, xch, red, bars, tcol,
                                zchunk, pc.zlo, pc.zhi, skip_last, pc.cfl_sum != 0);
     else
-        lead_group<T, COMP, 1, XT>(&tmap, g, f, scv, p, rk, err, cfl, smem, xch, red, bars, tcol,
+        lead_group<T, COMP, 1, XT, MODE>(&tmap, g, f, scv, p, rk, err, cfl, smem, xch, red, bars, tcol,
                                zchunk, pc.zlo, pc.zhi, skip_last, pc.cfl_sum != 0);
     /* no copy into this block's shared memory is left in flight */
     if (tid == 0)
@@ -1278,11 +1291,19 @@ launch_tiled(const Geom& g, const void* tmap_in, const FieldsT<T>& f, const Sten
          * per FP64 step, and in FP32 the second shared-memory buffer costs the
          * second block per SM: 24.9 against 27.5 ms) */
         const bool xt = k != AC_SOLVE_TILED_LEAD_ALT;
-        if (xt)
-            solve_lead_kernel<T, COMP, true><<<bpg, tpb, lead_smem_bytes<T, true>(), stream>>>(
-                *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err, cfl, zc);
+        /* substep 0 of the default kernel reads no previous state: its own form
+         * (measured at 512^3: 9.3 against 9.8 ms FP64, 6.2 against 6.7 ms FP32) */
+        const size_t sb = lead_smem_bytes<T, true>();
+        const CUtensorMap& tm = *(const CUtensorMap*)tmap_in;
+        const StencilT<T> st  = stencil_cast<T>(sc);
+        if (xt && rk.step == 0 && !cfl)
+            solve_lead_kernel<T, COMP, true, MODE_FIRST><<<bpg, tpb, sb, stream>>>(
+                tm, g, f, st, pc, rk, err, cfl, zc);
+        else if (xt)
+            solve_lead_kernel<T, COMP, true, MODE_RUNTIME><<<bpg, tpb, sb, stream>>>(
+                tm, g, f, st, pc, rk, err, cfl, zc);
         else
-            solve_lead_kernel<T, COMP, false><<<bpg, tpb, lead_smem_bytes<T, false>(), stream>>>(
+            solve_lead_kernel<T, COMP, false, MODE_RUNTIME><<<bpg, tpb, lead_smem_bytes<T, false>(), stream>>>(
                 *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err, cfl, zc);
     }
     else
@@ -1361,10 +1382,13 @@ ac_solve_tiled_init(const int precision)
             (e = set_smem<double>((const void*)solve_tiled_kernel<double, false, true>,
                                   L::SMEM_BYTES)) != cudaSuccess)
             return e;
-        if ((e = set_smem<double>((const void*)solve_lead_kernel<double, false, true>,
-                                  lead_smem_bytes<double, true>())) != cudaSuccess)
+        if ((e = set_smem<double>((const void*)solve_lead_kernel<double, false, true, MODE_FIRST>,
+                                  lead_smem_bytes<double, true>())) != cudaSuccess ||
+            (e = set_smem<double>(
+                 (const void*)solve_lead_kernel<double, false, true, MODE_RUNTIME>,
+                 lead_smem_bytes<double, true>())) != cudaSuccess)
             return e;
-        return set_smem<double>((const void*)solve_lead_kernel<double, false, false>,
+        return set_smem<double>((const void*)solve_lead_kernel<double, false, false, MODE_RUNTIME>,
                                 lead_smem_bytes<double, false>());
     }
     typedef Layout<float> L;
@@ -1373,10 +1397,12 @@ ac_solve_tiled_init(const int precision)
         (e = set_smem<float>((const void*)solve_tiled_kernel<float, true, true>, L::SMEM_BYTES)) !=
             cudaSuccess)
         return e;
-    if ((e = set_smem<float>((const void*)solve_lead_kernel<float, true, true>,
+    if ((e = set_smem<float>((const void*)solve_lead_kernel<float, true, true, MODE_FIRST>,
+                             lead_smem_bytes<float, true>())) != cudaSuccess ||
+        (e = set_smem<float>((const void*)solve_lead_kernel<float, true, true, MODE_RUNTIME>,
                              lead_smem_bytes<float, true>())) != cudaSuccess)
         return e;
-    return set_smem<float>((const void*)solve_lead_kernel<float, true, false>,
+    return set_smem<float>((const void*)solve_lead_kernel<float, true, false, MODE_RUNTIME>,
                            lead_smem_bytes<float, false>());
 }
 
