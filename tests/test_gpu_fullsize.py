@@ -1,5 +1,12 @@
-"""Parity at the benchmark's full size (512^3), where the CPU oracle is too
-slow, through size-independent properties; and a 256^3 step against the oracle.
+"""Parity at the benchmark's full size (512^3): one step against statistics of
+the reference's own host model committed as a fixture, and size-independent
+properties where the CPU oracle is too slow; and a 256^3 step against the
+oracle.
+
+* One FP64 RK3 step of the seeded benchmark mesh against golden_512.json
+  (tests/golden/make_golden_512.py, from the reference's host model): 1024
+  sampled cells within 1e-12 of each field's largest value, and the field
+  minima, maxima, sums and sums of squares.
 
 * Translation invariance: the update of every cell is the same arithmetic on
   the same values wherever the cell sits in the tiles, so integrating a
@@ -8,6 +15,10 @@ slow, through size-independent properties; and a 256^3 step against the oracle.
   breaks the equality.
 * FP32-compensated against FP64 at 512^3 after 5 steps within the 1e-5 bar.
 """
+import hashlib
+import json
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -41,6 +52,35 @@ def _steps(dev, torch, f, steps):
     for _ in range(steps):
         dev.integrate_step(DT)
     return dev.store_mesh_device(torch.empty_like(f))
+
+
+GOLDEN_512 = Path(__file__).resolve().parent / "golden" / "golden_512.json"
+
+
+def test_512_one_step_vs_reference_golden():
+    """One FP64 RK3 step at 512^3 (default kernel choice) against the reference's
+    host model: the statistics and sampled cells of tests/golden/golden_512.json."""
+    from tests.golden.make_golden_512 import stats
+
+    meta = json.loads(GOLDEN_512.read_text())
+    n = meta["n"]
+    info = ab.make_info(n, **ab.CONFIG_PARAMS)
+    f = ab.seeded_mesh(info, meta["seed"])
+    assert hashlib.sha256(f.tobytes()).hexdigest() == meta["input_sha256"]
+    with ab.Device(info) as dev:
+        dev.load_mesh(f)
+        dev.integrate_step(meta["dt"])
+        dev.synchronize()
+        got = dev.store_mesh(f)
+    s = stats(got, n)
+    for q in range(8):
+        scale = max(abs(meta["min"][q]), abs(meta["max"][q]))
+        err = np.abs(np.array(s["samples"][q]) - np.array(meta["samples"][q])).max() / scale
+        assert err <= 1e-12, (q, err)
+        assert abs(s["min"][q] - meta["min"][q]) <= 1e-12 * scale, q
+        assert abs(s["max"][q] - meta["max"][q]) <= 1e-12 * scale, q
+        assert abs(s["sum_sq"][q] - meta["sum_sq"][q]) <= 2e-12 * meta["sum_sq"][q], q
+        assert abs(s["sum"][q] - meta["sum"][q]) <= 1e-12 * meta["sum_abs"][q], q
 
 
 @pytest.mark.parametrize("shift", [(5, 37, 100), (1, 1, 1), (64, 4, 0)])
