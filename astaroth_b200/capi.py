@@ -278,6 +278,7 @@ SIGNATURES = {
                                                         C.POINTER(C.c_double)]),
     "acDeviceReduceVecScal": (C.c_int, [Device_p, C.c_int, AcReduction, C.c_int, C.c_int,
                                         C.c_int, C.c_int, C.POINTER(C.c_double)]),
+    "acDeviceGetReduceNonFinite": (C.c_int, [Device_p, C.POINTER(C.c_int)]),
     "acDeviceGetVertexBufferPtrs": (C.c_int, [Device_p, C.c_int,
                                               C.POINTER(C.POINTER(C.c_double)),
                                               C.POINTER(C.POINTER(C.c_double))]),

@@ -223,6 +223,21 @@ acB200Version(void)
     return kVersion;
 }
 
+/* Host-side fault injection for the failure-path tests.  With the environment
+ * variable AC_FAULT_INJECT set to
+ *   "create": acDeviceCreate fails before it allocates anything;
+ *   "alloc":  acDeviceCreate's second state allocation fails, after the first
+ *             succeeded, so its release path runs;
+ *   "launch": every substep launch fails,
+ * each as the CUDA call at that point would fail.  Unset, it costs one getenv
+ * per create and per substep launch. */
+static bool
+fault_at(const char* site)
+{
+    const char* v = getenv("AC_FAULT_INJECT");
+    return v && strcmp(v, site) == 0;
+}
+
 extern "C" AcResult
 acDeviceCreate(const int id, const AcMeshInfo device_config, Device* device_handle)
 {
@@ -236,6 +251,10 @@ acDeviceCreate(const int id, const AcMeshInfo device_config, Device* device_hand
         return AC_FAILURE;
     }
     AC_CUDA_CHECK(cudaSetDevice(id));
+    if (fault_at("create")) {
+        fprintf(stderr, "astaroth_b200: acDeviceCreate failed (AC_FAULT_INJECT=create)\n");
+        return AC_FAILURE;
+    }
 
     AcMeshInfo info = device_config;
     if (acHostUpdateParams(&info) != AC_SUCCESS) {
@@ -277,7 +296,8 @@ acDeviceCreate(const int id, const AcMeshInfo device_config, Device* device_hand
 
     const size_t bytes = (size_t)AC_NF * (size_t)d->geom.cells * elem_size(d);
     for (int b = 0; b < 2; ++b) {
-        CREATE_CHECK(cudaMalloc(&d->hi[b], bytes));
+        CREATE_CHECK(b == 1 && fault_at("alloc") ? cudaErrorMemoryAllocation
+                                                 : cudaMalloc(&d->hi[b], bytes));
         /* zero-filled in and out, as acVBAReset (acc-runtime/api/vba.cc:274-307) */
         CREATE_CHECK(cudaMemsetAsync(d->hi[b], 0, bytes, d->streams[0]));
         if (precision == 1) {
@@ -298,6 +318,7 @@ acDeviceCreate(const int id, const AcMeshInfo device_config, Device* device_hand
     CREATE_CHECK(cudaMalloc((void**)&d->red.partials, rbytes));
     CREATE_CHECK(cudaMemsetAsync(d->red.partials, 0, rbytes, d->streams[0]));
     d->red.result  = d->red.partials + 2 * (size_t)blocks;
+    d->red.nonfinite = (unsigned int*)(d->red.result + 1);
     d->red.counter = (unsigned int*)(d->red.result + 2);
     d->err_flag    = (int*)(d->red.counter + 4);
     d->cfl         = (unsigned long long*)(d->red.counter + 8);
@@ -305,7 +326,7 @@ acDeviceCreate(const int id, const AcMeshInfo device_config, Device* device_hand
                  ac_make_tensor_map(&d->tmap[1], d->hi[1], d->geom, precision);
     if (d->tmap_ok)
         CREATE_CHECK(ac_solve_tiled_init(precision));
-    CREATE_CHECK(cudaMallocHost((void**)&d->host_result, sizeof(double)));
+    CREATE_CHECK(cudaMallocHost((void**)&d->host_result, 2 * sizeof(double)));
     CREATE_CHECK(ensure_bfield(d));
     CREATE_CHECK(cudaStreamSynchronize(d->streams[0]));
 #undef CREATE_CHECK
@@ -712,6 +733,8 @@ cudaError_t
 launch_substep(Device d, cudaStream_t st, const int step, const double dt,
                unsigned long long* launches, const int zlo, const int zhi)
 {
+    if (fault_at("launch"))
+        return cudaErrorLaunchFailure;
     StencilCoef sc;
     PhysConst pc;
     ac_make_stencil(d->config, &sc);
@@ -890,13 +913,20 @@ acDeviceIntegrateStep(const Device d, const Stream stream, const AcReal dt)
         if (sg.valid)
             cudaGraphExecDestroy(sg.exec);
         sg.valid = 0;
-        cudaGraph_t graph;
+        cudaGraph_t graph = nullptr;
+        int in_idx[AC_NF];
+        memcpy(in_idx, d->in_idx, sizeof(in_idx));
         AC_CUDA_CHECK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
         const cudaError_t rec = record_step(d, st, dt, NULL);
         const cudaError_t end = cudaStreamEndCapture(st, &graph);
-        acDeviceSwapBuffers(d); /* undo the capture's swaps (three swaps = one) */
-        AC_CUDA_CHECK(rec);
-        AC_CUDA_CHECK(end);
+        /* the capture's swaps (three on success, fewer when a launch failed) undone */
+        memcpy(d->in_idx, in_idx, sizeof(in_idx));
+        if (rec != cudaSuccess || end != cudaSuccess) {
+            if (graph)
+                cudaGraphDestroy(graph);
+            AC_CUDA_CHECK(rec);
+            AC_CUDA_CHECK(end);
+        }
         const cudaError_t inst = cudaGraphInstantiate(&sg.exec, graph, 0);
         cudaGraphDestroy(graph);
         AC_CUDA_CHECK(inst);
@@ -951,12 +981,17 @@ reduce_common(const Device d, const Stream stream, const AcReduction r, const in
         }
     }
     cudaStream_t st = d->streams[stream];
+    AC_CUDA_CHECK(cudaMemsetAsync(d->red.nonfinite, 0, sizeof(unsigned int), st));
     AC_CUDA_CHECK(ac_launch_reduce(d->geom, fp, lo, kind, d->precision, map, r.reduce_op, d->red,
                                    st, &d->launches));
-    AC_CUDA_CHECK(cudaMemcpyAsync(d->host_result, d->red.result, sizeof(double),
+    /* the result and the non-finite flag behind it */
+    AC_CUDA_CHECK(cudaMemcpyAsync(d->host_result, d->red.result, 2 * sizeof(double),
                                   cudaMemcpyDeviceToHost, st));
     AC_CUDA_CHECK(cudaStreamSynchronize(st));
-    *result = *d->host_result;
+    *result           = d->host_result[0];
+    unsigned int flag = 0;
+    memcpy(&flag, &d->host_result[1], sizeof(flag));
+    d->last_nonfinite = flag != 0;
     return AC_SUCCESS;
 }
 
@@ -977,6 +1012,18 @@ acDeviceReduceScalNoPostProcessing(const Device d, const Stream stream, const Ac
                                    const VertexBufferHandle h, AcReal* result)
 {
     return reduce_common(d, stream, r, 1, &h, result);
+}
+
+/* Whether the last acDeviceReduce* call on this device met a mapped value that
+ * was NaN or infinite (a maximum or minimum drops NaN, so the value alone does
+ * not show it). */
+extern "C" AcResult
+acDeviceGetReduceNonFinite(const Device d, int* nonfinite)
+{
+    if (!d || !nonfinite)
+        return AC_FAILURE;
+    *nonfinite = d->last_nonfinite;
+    return AC_SUCCESS;
 }
 
 extern "C" AcResult

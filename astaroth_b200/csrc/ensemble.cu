@@ -675,6 +675,7 @@ acEnsembleCreate(const int device_id, const int n, const AcMeshInfo* member_info
     ENS_CHECK(cudaMemsetAsync(e->red.partials, 0, rbytes, e->stream));
     e->red.result  = e->red.partials + 2 * (size_t)max_blocks;
     e->red.counter = (unsigned int*)(e->red.result + 2);
+    e->red.nonfinite = nullptr;
     ENS_CHECK(cudaMallocHost((void**)&e->host_result, sizeof(double)));
     ENS_CHECK(cudaStreamSynchronize(e->stream));
     const AcEnsembleTiles def = {32, 4, 8, 0, 0};

@@ -124,9 +124,11 @@ typedef FieldsT<float> Fields32;
 /* Scratch of the reductions: per-block partials, a completion counter and
  * the device-side result. */
 struct ReduceScratch {
-    double* partials;      /* 2 doubles per block */
-    unsigned int* counter; /* zero between calls */
-    double* result;        /* 1 double */
+    double* partials;        /* 2 doubles per block */
+    unsigned int* counter;   /* zero between calls */
+    double* result;          /* 1 double, then the non-finite flag (result + 1) */
+    unsigned int* nonfinite; /* the low word of result[1]: 1 when a mapped value was NaN or
+                              * infinite; cleared before each call (may be null) */
     int max_blocks;
 };
 
@@ -170,6 +172,7 @@ struct device_s {
     StepGraph graphs[NUM_STREAMS][2];
     int solve_variant;   /* 0 = plain, else the tiled kernel AC_SOLVE_TILED_* */
     int debug_skip_load; /* acDeviceDebugSkipPlaneLoad */
+    int last_nonfinite;  /* the last reduction met a NaN or infinite mapped value */
     /* planes of substep 2 solved since the CFL maxima were last cleared (a
      * substep solved in z boxes clears them once, at its first box) */
     int cfl_cover;

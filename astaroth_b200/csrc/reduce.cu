@@ -109,11 +109,13 @@ combine(const int op, const double a, const double b)
     return op == AC_REDUCE_OP_MAX ? fmax(a, b) : fmin(a, b);
 }
 
+/* nonfinite (optional): set to 1 when a mapped value is NaN or infinite, which a
+ * maximum or minimum would otherwise hide (fmax and fmin drop NaN) */
 template <typename R>
 __global__ void __launch_bounds__(kTpb)
 reduce_kernel(const Geom g, const R f, const int map, const int op,
               double* __restrict__ partials, unsigned int* __restrict__ counter,
-              double* __restrict__ result)
+              double* __restrict__ result, unsigned int* __restrict__ nonfinite)
 {
     __shared__ double s_hi[kTpb / 32];
     __shared__ double s_lo[kTpb / 32];
@@ -123,6 +125,7 @@ reduce_kernel(const Geom g, const R f, const int map, const int op,
 
     DD acc{0.0, 0.0};
     double ext          = ident;
+    bool bad            = false;
     const long long rows = (long long)g.ny * g.nz;
     for (long long r = blockIdx.x; r < rows; r += gridDim.x) {
         const int j          = (int)(r % g.ny);
@@ -130,12 +133,15 @@ reduce_kernel(const Geom g, const R f, const int map, const int op,
         const long long base = geom_idx(g, NGHOST, j + NGHOST, k + NGHOST);
         for (int i = threadIdx.x; i < g.nx; i += kTpb) {
             const double v = map_value(map, f, base + i);
+            bad |= !isfinite(v);
             if (is_sum)
                 acc = dd_add(acc, v);
             else
                 ext = combine(op, ext, v);
         }
     }
+    if (__syncthreads_or(bad) && nonfinite && threadIdx.x == 0)
+        atomicOr(nonfinite, 1u);
     /* warp */
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
@@ -240,7 +246,8 @@ ac_launch_reduce(const Geom& g, const void* const* fields, const float* const* l
         for (int q = 0; q < 4; ++q)
             f.p[q] = (const double*)fields[q < nfields ? q : 0];
         reduce_kernel<<<blocks, kTpb, 0, stream>>>(g, f, map, op, scratch.partials,
-                                                   scratch.counter, scratch.result);
+                                                   scratch.counter, scratch.result,
+                                                   scratch.nonfinite);
     }
     else {
         ReaderComp f;
@@ -249,7 +256,8 @@ ac_launch_reduce(const Geom& g, const void* const* fields, const float* const* l
             f.lo[q] = lo[q < nfields ? q : 0];
         }
         reduce_kernel<<<blocks, kTpb, 0, stream>>>(g, f, map, op, scratch.partials,
-                                                   scratch.counter, scratch.result);
+                                                   scratch.counter, scratch.result,
+                                                   scratch.nonfinite);
     }
     if (launches)
         ++*launches;
@@ -373,7 +381,7 @@ acReduceNoAlloc(const AcReal* const* fields, const int nfields, const int nx, co
     Reader64 f;
     for (int q = 0; q < 4; ++q)
         f.p[q] = fields[q < nfields ? q : 0];
-    reduce_kernel<<<nb, kTpb, 0, st>>>(g, f, map, op, partials, counter, result);
+    reduce_kernel<<<nb, kTpb, 0, st>>>(g, f, map, op, partials, counter, result, nullptr);
     AC_CUDA_CHECK(cudaGetLastError());
     return AC_SUCCESS;
 }

@@ -249,6 +249,13 @@ class Device:
                "acDeviceReduceVecScal")
         return out.value
 
+    def reduce_nonfinite(self) -> bool:
+        """Whether the last reduction met a NaN or infinite value (after its map)."""
+        v = C.c_int()
+        _check(self.lib.acDeviceGetReduceNonFinite(self._h, C.byref(v)),
+               "acDeviceGetReduceNonFinite")
+        return bool(v.value)
+
     # ---- CFL timestep (computed by substep 2, or by calc_timestep) ----
     def calc_timestep(self, stream: int = 0) -> None:
         _check(self.lib.acDeviceCalcTimestep(self._h, stream), "acDeviceCalcTimestep")
