@@ -1287,9 +1287,9 @@ launch_tiled(const Geom& g, const void* tmap_in, const FieldsT<T>& f, const Sten
             *(const CUtensorMap*)tmap_in, g, f, stencil_cast<T>(sc), pc, rk, err, cfl, zc);
     else if (k == AC_SOLVE_TILED_LEAD || k == AC_SOLVE_TILED_LEAD_ALT) {
         /* the exchange between the warp groups goes through tensor memory; _ALT
-         * takes shared memory instead (measured at 512^3: 33.6 against 34.2 ms
+         * takes shared memory instead (measured at 512^3: 28.5 against 29.5 ms
          * per FP64 step, and in FP32 the second shared-memory buffer costs the
-         * second block per SM: 24.9 against 27.5 ms) */
+         * second block per SM: 22.8 against 32.0 ms) */
         const bool xt = k != AC_SOLVE_TILED_LEAD_ALT;
         /* substep 0 of the default kernel reads no previous state: its own form
          * (measured at 512^3: 9.3 against 9.8 ms FP64, 6.2 against 6.7 ms FP32) */
