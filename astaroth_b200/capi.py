@@ -312,6 +312,9 @@ SIGNATURES = {
     "acDevicePlaneBytes": (C.c_size_t, [Device_p]),
     "acDevicePackPlanes": (C.c_int, [Device_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
     "acDeviceUnpackPlanes": (C.c_int, [Device_p, C.c_int, C.c_int, C.c_int, C.c_void_p]),
+    "acDeviceBoxBytes": (C.c_size_t, [Device_p, Int3]),
+    "acDevicePackBox": (C.c_int, [Device_p, C.c_int, Int3, Int3, C.c_void_p]),
+    "acDeviceUnpackBox": (C.c_int, [Device_p, C.c_int, Int3, Int3, C.c_void_p]),
     "acDeviceWriteMeshToDisk": (C.c_int, [Device_p, C.c_char_p, C.c_char_p, C.c_int]),
     "acDeviceReadMeshFromDisk": (C.c_int, [Device_p, C.c_char_p, C.c_char_p, C.c_int]),
     "acDeviceAdjointTapeForward": (C.c_int, [Device_p, C.c_int, C.c_int, C.c_double]),

@@ -331,6 +331,34 @@ planes_kernel(const PlaneArrays arr, const int narrays, const long long offset,
     }
 }
 
+/* A box of every array <-> the packed buffer (array-major, then z, y, x), the
+ * reference's kernel_pack_data / kernel_unpack_data
+ * (src/core/kernels/packing.cuh:59-90,133-160) for one element type E. */
+template <typename E>
+__global__ void
+box_kernel(const PlaneArrays arr, const int narrays, const long long px, const long long pxy,
+           const int3 start, const int3 dims, E* __restrict__ buffer, const bool pack)
+{
+    const long long row   = dims.x;
+    const long long cells = row * dims.y * dims.z;
+    const long long total = (long long)narrays * cells;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int a         = (int)(t / cells);
+        const long long c   = t - (long long)a * cells;
+        const long long r   = c / row; /* row index within the box: j + dims.y * k */
+        const int i         = (int)(c - r * row);
+        const int j         = (int)(r % dims.y);
+        const int k         = (int)(r / dims.y);
+        E* f = reinterpret_cast<E*>(arr.a[a]) + (start.x + i) + (long long)(start.y + j) * px +
+               (long long)(start.z + k) * pxy;
+        if (pack)
+            buffer[t] = *f;
+        else
+            *f = buffer[t];
+    }
+}
+
 /* dst = src for n2 double2 pairs (both 16-byte aligned), grid-stride */
 __global__ void
 copy2_kernel(const double2* __restrict__ src, double2* __restrict__ dst, const long long n2)
@@ -465,6 +493,34 @@ ac_launch_planes(void* const* arrays, const int narrays, const long long offset_
     const long long count = bytes / 8;
     planes_kernel<<<grid_for((long long)narrays * count, 256), 256, 0, stream>>>(
         arr, narrays, offset_bytes / 8, count, (unsigned long long*)buffer, pack);
+    if (launches)
+        ++*launches;
+    return cudaGetLastError();
+}
+
+cudaError_t
+ac_launch_box(void* const* arrays, const int narrays, const size_t elem, const Geom& g,
+              const int3 start, const int3 dims, void* buffer, const bool pack,
+              cudaStream_t stream, unsigned long long* launches)
+{
+    if (narrays < 1 || narrays > 2 * AC_NF || (elem != 4 && elem != 8) ||
+        ((uintptr_t)buffer & (elem - 1)) || dims.x < 1 || dims.y < 1 || dims.z < 1 ||
+        start.x < 0 || start.y < 0 || start.z < 0 || start.x + dims.x > g.mx ||
+        start.y + dims.y > g.my || start.z + dims.z > g.mz)
+        return cudaErrorInvalidValue;
+    PlaneArrays arr;
+    for (int a = 0; a < narrays; ++a) {
+        if ((uintptr_t)arrays[a] & (elem - 1))
+            return cudaErrorInvalidValue;
+        arr.a[a] = (unsigned long long*)arrays[a];
+    }
+    const long long total = (long long)narrays * dims.x * dims.y * dims.z;
+    if (elem == 8)
+        box_kernel<unsigned long long><<<grid_for(total, 256), 256, 0, stream>>>(
+            arr, narrays, g.px, g.pxy, start, dims, (unsigned long long*)buffer, pack);
+    else
+        box_kernel<unsigned int><<<grid_for(total, 256), 256, 0, stream>>>(
+            arr, narrays, g.px, g.pxy, start, dims, (unsigned int*)buffer, pack);
     if (launches)
         ++*launches;
     return cudaGetLastError();

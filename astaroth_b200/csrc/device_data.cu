@@ -405,6 +405,19 @@ acDevicePlaneBytes(const Device d)
     return d ? (size_t)d->geom.pxy * elem_size(d) * plane_arrays(d) : 0;
 }
 
+/* the in-buffer arrays in packing order: the 8 fields, then (FP32-compensated)
+ * their 8 compensation arrays */
+static void
+packing_arrays(const Device d, void* arrays[2 * AC_NF])
+{
+    const size_t es = elem_size(d);
+    for (int a = 0; a < plane_arrays(d); ++a) {
+        const int q = a % AC_NF;
+        arrays[a]   = a < AC_NF ? (void*)((char*)d->hi[d->in_idx[q]] + (size_t)q * d->geom.cells * es)
+                                : (void*)arr_lo(d, d->in_idx[q], q);
+    }
+}
+
 static AcResult
 copy_planes(const Device d, const Stream stream, const int z0, const int nplanes, char* buffer,
             const bool pack)
@@ -414,11 +427,7 @@ copy_planes(const Device d, const Stream stream, const int z0, const int nplanes
     AC_CUDA_CHECK(cudaSetDevice(d->id));
     const size_t es = elem_size(d);
     void* arrays[2 * AC_NF];
-    for (int a = 0; a < plane_arrays(d); ++a) {
-        const int q = a % AC_NF;
-        arrays[a]   = a < AC_NF ? (void*)((char*)d->hi[d->in_idx[q]] + (size_t)q * d->geom.cells * es)
-                                : (void*)arr_lo(d, d->in_idx[q], q);
-    }
+    packing_arrays(d, arrays);
     /* one launch for all arrays (the buffer holds array a at a * bytes) */
     AC_CUDA_CHECK(ac_launch_planes(arrays, plane_arrays(d), (long long)z0 * d->geom.pxy * es,
                                    (long long)nplanes * d->geom.pxy * es, buffer, pack,
@@ -438,6 +447,57 @@ acDeviceUnpackPlanes(const Device d, const Stream stream, const int z0, const in
                      const void* buffer)
 {
     return copy_planes(d, stream, z0, nplanes, (char*)buffer, false);
+}
+
+/* ---- box copies for a decomposition in x, y and z ----
+ * The faces of a decomposition in x or y are strided in every array: one
+ * launch gathers the box [start, start + dims) (padded mesh indices) of every
+ * array into the buffer, array by array, then z, y, x (x fastest), as the
+ * reference's kernel_pack_data does (src/core/kernels/packing.cuh:59-90);
+ * unpack scatters it back (kernel_unpack_data, packing.cuh:133-160). */
+static bool
+box_ok(const Device d, const int3 start, const int3 dims)
+{
+    const Geom& g = d->geom;
+    return dims.x > 0 && dims.y > 0 && dims.z > 0 && start.x >= 0 && start.y >= 0 &&
+           start.z >= 0 && (long long)start.x + dims.x <= g.mx &&
+           (long long)start.y + dims.y <= g.my && (long long)start.z + dims.z <= g.mz;
+}
+
+extern "C" size_t
+acDeviceBoxBytes(const Device d, const int3 dims)
+{
+    if (!d || dims.x <= 0 || dims.y <= 0 || dims.z <= 0)
+        return 0;
+    return (size_t)dims.x * dims.y * dims.z * elem_size(d) * plane_arrays(d);
+}
+
+static AcResult
+copy_box(const Device d, const Stream stream, const int3 start, const int3 dims, void* buffer,
+         const bool pack)
+{
+    if (!d || !box_ok(d, start, dims) || !buffer || !stream_ok(stream))
+        return AC_FAILURE;
+    AC_CUDA_CHECK(cudaSetDevice(d->id));
+    void* arrays[2 * AC_NF];
+    packing_arrays(d, arrays);
+    AC_CUDA_CHECK(ac_launch_box(arrays, plane_arrays(d), elem_size(d), d->geom, start, dims,
+                                buffer, pack, d->streams[stream], &d->launches));
+    return AC_SUCCESS;
+}
+
+extern "C" AcResult
+acDevicePackBox(const Device d, const Stream stream, const int3 start, const int3 dims,
+                void* buffer)
+{
+    return copy_box(d, stream, start, dims, buffer, true);
+}
+
+extern "C" AcResult
+acDeviceUnpackBox(const Device d, const Stream stream, const int3 start, const int3 dims,
+                  const void* buffer)
+{
+    return copy_box(d, stream, start, dims, (void*)buffer, false);
 }
 
 /* ---- snapshots of the computational domain: src/core/grid.cc:3792-3935 ----

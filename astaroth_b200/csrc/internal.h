@@ -220,6 +220,13 @@ cudaError_t ac_launch_fill(double* ptr, const long long count, const double valu
 cudaError_t ac_launch_planes(void* const* arrays, const int narrays, const long long offset_bytes,
                              const long long bytes, void* buffer, const bool pack,
                              cudaStream_t stream, unsigned long long* launches);
+/* Pack (or unpack) the box [start, start + dims) of each of narrays (<= 16)
+ * arrays of geometry g, elements of `elem` bytes (4 or 8), into (from) buffer,
+ * array-major then z, y, x; one launch.  Boxes outside the padded mesh are
+ * refused (cudaErrorInvalidValue). */
+cudaError_t ac_launch_box(void* const* arrays, const int narrays, const size_t elem, const Geom& g,
+                          const int3 start, const int3 dims, void* buffer, const bool pack,
+                          cudaStream_t stream, unsigned long long* launches);
 /* Host-layout linear range [first, first + count) of one field: doubles at
  * those indices of src/dst <-> (hi, lo) in the FP32 device layout. */
 cudaError_t ac_launch_split_range(const Geom& g, const double* src, float* hi, float* lo,

@@ -115,6 +115,60 @@ def test_grid_halo_exchange_gloo(world):
         assert (mx, mn, sm) == (world, 1, world * (world + 1) / 2)
 
 
+def _grid_exchange_worker(rank, world, port, dims, mapping, out):
+    import torch
+
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    assert adist.init("gloo", timeout_s=60)
+    from astaroth_b200.grid import DistTransport, ProcessGrid
+
+    t = DistTransport()
+    pg = ProcessGrid((24, 24, 24), dims, mapping)
+    res = []
+    for _ in range(2):  # repeated rounds keep matching in order
+        for axis in range(3):
+            sb = torch.full((16,), 100 * rank + 10 * axis + 1, dtype=torch.int32)
+            st = torch.full((16,), 100 * rank + 10 * axis + 2, dtype=torch.int32)
+            rb = torch.zeros(16, dtype=torch.int32)
+            rt = torch.zeros(16, dtype=torch.int32)
+            t.exchange([sb], [st], [rb], [rt], lo=[pg.neighbour(rank, axis, -1)],
+                       hi=[pg.neighbour(rank, axis, +1)], tag=axis)
+            res.append((axis, int(rb[0]), int(rb[-1]), int(rt[0]), int(rt[-1])))
+    out.put((rank, res))
+    adist.barrier()
+    adist.destroy()
+
+
+@pytest.mark.parametrize("dims,mapping", [((2, 2, 1), "linear"), ((1, 2, 2), "morton"),
+                                          ((2, 1, 2), "linear")])
+def test_process_grid_exchange_gloo(dims, mapping):
+    """Along each axis of a 4-rank process grid, a rank's low ghost receives
+    the high cells of its neighbour below and its high ghost the low cells of
+    the one above; an axis that is not split exchanges with itself; the tags
+    keep the three axes apart."""
+    from astaroth_b200.grid import ProcessGrid
+
+    world = 4
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_grid_exchange_worker, args=(r, world, port, dims, mapping, q))
+             for r in range(world)]
+    for p in procs:
+        p.start()
+    res = dict(q.get(timeout=120) for _ in range(world))
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    pg = ProcessGrid((24, 24, 24), dims, mapping)
+    for rank, rows in res.items():
+        for axis, rb0, rb1, rt0, rt1 in rows:
+            below, above = pg.neighbour(rank, axis, -1), pg.neighbour(rank, axis, +1)
+            assert rb0 == rb1 == 100 * below + 10 * axis + 2
+            assert rt0 == rt1 == 100 * above + 10 * axis + 1
+
+
 def test_decompose_covers_the_planes():
     from astaroth_b200.grid import decompose
 

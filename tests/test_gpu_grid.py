@@ -176,6 +176,101 @@ def test_forcing_across_slabs():
     assert err <= 1e-13
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_pack_unpack_box(precision):
+    """acDevicePackBox gathers a box of every array (x fastest), acDeviceUnpackBox
+    scatters it into another device at the same place and nowhere else; boxes
+    outside the padded mesh are refused."""
+    import torch
+
+    lib = capi.load()
+    info = make_info((20, 16, 12), precision=precision)
+    f = seeded_mesh(info, 90)
+    start, size = capi.Int3(2, 5, 4), capi.Int3(7, 3, 9)
+    with Device(info) as a, Device(info) as b:
+        a.load_mesh(f)
+        b.load_mesh(np.zeros_like(f))
+        nbytes = lib.acDeviceBoxBytes(a.handle, size)
+        assert nbytes == 7 * 3 * 9 * 8 * 8  # 8 fields of 8 B, or 16 arrays of 4 B
+        buf = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+        assert lib.acDevicePackBox(a.handle, 0, start, size, buf.data_ptr()) == capi.AC_SUCCESS
+        assert lib.acDeviceUnpackBox(b.handle, 0, start, size, buf.data_ptr()) == capi.AC_SUCCESS
+        a.synchronize()
+        b.synchronize()
+        got = b.store_mesh()
+        if precision == 0:
+            packed = buf.cpu().numpy().view(np.float64).reshape(8, 9, 3, 7)
+            assert np.array_equal(packed, f[:, 4:13, 5:8, 2:9])
+        box = np.zeros(got.shape, dtype=bool)
+        box[:, 4:13, 5:8, 2:9] = True
+        assert np.array_equal(got[box], a.store_mesh()[box])
+        assert not got[~box].any()
+        for st, sz in (((-1, 0, 0), (3, 3, 3)), ((0, 0, 0), (27, 1, 1)), ((0, 20, 0), (1, 3, 1)),
+                       ((0, 0, 0), (0, 1, 1))):
+            assert lib.acDevicePackBox(a.handle, 0, capi.Int3(*st), capi.Int3(*sz),
+                                       buf.data_ptr()) == capi.AC_FAILURE
+        assert lib.acDeviceBoxBytes(a.handle, capi.Int3(0, 4, 4)) == 0
+
+
+# process grids: x, y and z split, ranks linear or in the reference's Morton order
+PENCILS = [((2, 1, 1), "linear"), ((1, 2, 1), "linear"), ((2, 2, 1), "linear"),
+           ((2, 2, 2), "morton"), ((1, 3, 2), "linear"), ("morton", None)]
+
+
+@pytest.mark.parametrize("kernel", [0, 3])
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("decomp,mapping", PENCILS)
+def test_pencils_equal_one_device(decomp, mapping, precision, kernel):
+    """A mesh split in x, y and z (the three-pass exchange of acDevicePackBox /
+    acDeviceUnpackBox) gives the bits of one undecomposed Device.  Every
+    sub-domain is at least one 32-cell tile wide, so the kernel of the whole
+    mesh runs on every sub-domain too (narrower meshes take the plain kernel)."""
+    info = make_info((64, 40, 30), precision=precision)
+    info.int_params[IntParam.AC_debug_plain_kernel] = kernel
+    f = seeded_mesh(info, 91, sigma_uu=1e-2)
+    kw = dict(decomp=decomp, slabs=4) if mapping is None else dict(decomp=decomp, mapping=mapping)
+    with Grid(info, **kw) as g:
+        assert not g.slabs_only and not g.overlap
+        g.load_mesh(f)
+        for _ in range(3):
+            g.integrate_step(DT)
+        g.synchronize()
+        got = g.store_mesh()
+    assert np.array_equal(_interior(got), _interior(_device(info, f, 3)))
+
+
+def test_pencils_reductions_timestep_and_forcing():
+    """Reductions and the CFL timestep of a (2, 2, 2) grid equal one Device's;
+    with forcing on, the phase of each block is shifted by its x, y and z
+    offsets."""
+    info = make_info((64, 40, 30))
+    f = seeded_mesh(info, 92, sigma_uu=1e-2)
+    with Grid(info, decomp=(2, 2, 2)) as g, Device(info) as d:
+        g.load_mesh(f)
+        d.load_mesh(f)
+        g.integrate_step(DT)
+        d.integrate_step(DT)
+        for rt in ("RTYPE_MAX", "RTYPE_MIN"):
+            assert g.reduce_scal(rt, 2) == d.reduce_scal(rt, 2)
+            assert g.reduce_vec(rt, 1, 2, 3) == d.reduce_vec(rt, 1, 2, 3)
+        for rt in ("RTYPE_RMS", "RTYPE_SUM", "RTYPE_RMS_EXP"):
+            assert g.reduce_scal(rt, 0) == pytest.approx(d.reduce_scal(rt, 0), rel=1e-13)
+        assert g.timestep() == d.timestep()
+    info = make_info((32, 32, 24), **dict(CONFIG_PARAMS, relhel=0.5, forcing_magnitude=0.5,
+                                           kmin=0.8, kmax=2.2, current_time=1.0))
+    info.int_params[IntParam.AC_lforcing] = 1
+    assert capi.load().acHostForcingParams(Real3(1, 0, 1), 0.4, 0.7, C.byref(info)) == 0
+    f = seeded_mesh(info, 93)
+    with Grid(info, decomp=(2, 2, 1)) as g:
+        g.load_mesh(f)
+        g.integrate_step(DT)
+        g.synchronize()
+        got = g.store_mesh()
+    ref = _device(info, f, 1)
+    err = np.abs(_interior(got) - _interior(ref)).max() / np.abs(_interior(ref)).max()
+    assert err <= 1e-13
+
+
 def test_dist_transport_one_rank():
     import torch.distributed as dist
 
