@@ -45,8 +45,8 @@ Transports:
   exchange is device-to-device copies.  It exercises the decomposition on one
   GPU and gives the same bits as an undecomposed Device.
 * ``DistTransport`` -- one sub-domain per rank of a torch.distributed process
-  group (NCCL between GPUs, gloo on CPU tensors): point-to-point sends of the
-  packed faces to the neighbouring ranks.
+  group (NCCL between GPUs, gloo on CPU tensors): the packed faces go to the
+  neighbouring ranks as one batch of point-to-point operations per exchange.
 
 Reductions combine the sub-domains' unprocessed results (max, min, sum) and
 apply the RMS post-processing with the global cell count; the CFL maxima are
@@ -268,6 +268,9 @@ class DistTransport:
         self.dist = dist
         self.rank = dist.get_rank()
         self.world = dist.get_world_size()
+        # every rank takes part in the group's first collective, so that the
+        # exchanges, which involve neighbours only, are never the first
+        dist.barrier()
 
     def exchange(self, send_bottom, send_top, recv_bottom, recv_top, streams=None, lo=None,
                  hi=None, tag=0):
@@ -289,9 +292,11 @@ class DistTransport:
             return
         d = self.dist
         t_up, t_down = 2 * tag + 1, 2 * tag + 2
-        reqs = [d.isend(st, up, tag=t_up), d.irecv(rb, down, tag=t_up),
-                d.isend(sb, down, tag=t_down), d.irecv(rt, up, tag=t_down)]
-        for r in reqs:
+        # one batch: a single NCCL group (ncclGroupStart / ncclSend, ncclRecv /
+        # ncclGroupEnd) for the four transfers
+        ops = [d.P2POp(d.isend, st, up, tag=t_up), d.P2POp(d.irecv, rb, down, tag=t_up),
+               d.P2POp(d.isend, sb, down, tag=t_down), d.P2POp(d.irecv, rt, up, tag=t_down)]
+        for r in d.batch_isend_irecv(ops):
             r.wait()
 
     def combine(self, values, op):
