@@ -3,7 +3,8 @@
  * ranges between host and device and between devices (the reference's
  * *WithOffset and acDeviceTransfer* family), volume copies, pipelined staged
  * loads, transfers from and to caller-owned device arrays, whole-plane
- * packing for slab decompositions, snapshots, and the auxiliary B field.
+ * packing for slab decompositions, box packing for decompositions in x, y and
+ * z, snapshots, and the auxiliary B field.
  */
 #include <errno.h>
 #include <math.h>
