@@ -45,7 +45,7 @@ constexpr int TX     = 32;
 constexpr int TY     = 4;
 constexpr int HY     = TY + 2 * NGHOST;
 constexpr int RING   = 8;
-constexpr int ZCHUNK = 256; /* the longest z chunk (zchunk_for) */
+constexpr int ZCHUNK = 512; /* the longest z chunk (zchunk_for) */
 constexpr int NCELL  = TX * TY; /* cells per tile, one per thread of a group */
 constexpr int XCHG   = (AC_H2M_COUNT + AC_M2H_COUNT) * NCELL; /* exchange entries */
 
@@ -1226,12 +1226,13 @@ encode_fn()
 
 /* Planes per CTA.  Every chunk reads and forms 6 halo planes beyond its own,
  * so long chunks are cheaper, until the grid quantises badly into waves of
- * resident CTAs.  Among 256, 128, 64 and 32 planes that keep at least two CTAs
- * per SM of the 148, the chunk with the least (waves of `per_sm` resident CTAs
- * per SM) x (planes a CTA steps through) is taken; the larger on a tie.
+ * resident CTAs.  Among 512, 256, 128, 64 and 32 planes that keep at least two
+ * CTAs per SM of the 148, the chunk with the least (waves of `per_sm` resident
+ * CTAs per SM) x (planes a CTA steps through) is taken; the larger on a tie.
  * Smaller grids halve 32 down to 8 while there are fewer than two CTAs per SM.
- * (Measured at 512^3, FP64: 256 planes 29.3 ms per step, 128 planes 29.6-29.8,
- * 64 planes 30.9; at 256^3, 256-plane chunks would leave 512 CTAs, 3.5 waves.) */
+ * (Measured at 512^3, FP64: 512 planes 28.9-29.1 ms per step against 29.2-29.3
+ * with 256; earlier 256 planes 29.3, 128 planes 29.6-29.8, 64 planes 30.9; at
+ * 256^3, 256-plane chunks would leave 512 CTAs, 3.5 waves.) */
 int
 zchunk_for(const Geom& g, const int nz, const int per_sm)
 {
