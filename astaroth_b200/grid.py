@@ -349,7 +349,13 @@ class Grid:
         self.slabs_only = self.pgrid.dims[0] == self.pgrid.dims[1] == 1
         # (z0, nz) of each local sub-domain
         self.ranges = [(off[2], n[2]) for off, n in self.boxes]
-        self.devs = [Device(subdomain_info(info, off, n), device_id) for off, n in self.boxes]
+        self.devs = []
+        try:
+            for off, n in self.boxes:
+                self.devs.append(Device(subdomain_info(info, off, n), device_id))
+        except BaseException:
+            self.destroy()  # the sub-domains made so far
+            raise
         self.plane_bytes = self.lib.acDevicePlaneBytes(self.devs[0].handle)
         dev = torch.device("cuda", device_id)
         self._dev = dev

@@ -3,7 +3,8 @@ order and default grids (src/core/decomposition/decomposition.cc:502-663), the
 tiling of the mesh by sub-domains, and the three-pass halo exchange plan
 (face_boxes along x, y, z with the neighbours of ProcessGrid), applied with
 numpy to every sub-domain of a random mesh: every ghost cell must equal the
-global periodic wrap."""
+global periodic wrap.  Also the Grid's clean-up when a sub-domain's Device
+cannot be made."""
 import numpy as np
 import pytest
 
@@ -122,3 +123,25 @@ def test_face_boxes_shapes():
     z = face_boxes(2, n)
     assert all(b[1] == (m[0], m[1], 3) for b in z)  # whole planes
     assert [b[0][2] for b in z] == [3, 6, 0, 9]
+
+
+def test_grid_releases_devices_when_one_fails(monkeypatch):
+    """A sub-domain whose Device cannot be made releases the ones made before it."""
+    import astaroth_b200.grid as grid
+    from astaroth_b200.device import make_info
+
+    made, destroyed = [], []
+
+    class FakeDevice:
+        def __init__(self, info, device_id=0):
+            if len(made) == 1:
+                raise RuntimeError("no device")
+            made.append(self)
+
+        def destroy(self):
+            destroyed.append(self)
+
+    monkeypatch.setattr(grid, "Device", FakeDevice)
+    with pytest.raises(RuntimeError):
+        grid.Grid(make_info((32, 32, 24)), decomp=(2, 1, 1))
+    assert len(made) == 1 and destroyed == made
